@@ -1,0 +1,418 @@
+"""Device programs over the C ABI (include/gaffa_b200.h).
+
+Each class owns the library's program handle (device metadata) and allocates
+its work buffers with torch on the program's device; torch is only the
+allocator and stream provider here -- every computation is a gf_* call into
+libgaffa_b200.so.  All calls are stream-ordered on the current torch stream
+and never synchronise implicitly, except where a host result is returned.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, ptr
+
+
+def _stream(stream=None):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _require_cuda(device_id: int) -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("gaffa_b200 needs a CUDA device (no CPU fallback)")
+    if device_id < 0 or device_id >= torch.cuda.device_count():
+        raise ValueError(f"device_id {device_id} out of range")
+    return torch.device("cuda", device_id)
+
+
+# ---------------------------------------------------------------------------
+# FFA plan (host)
+# ---------------------------------------------------------------------------
+
+class FfaPlan:
+    """Riptide FFA plan: tasks (TASK_DTYPE records) and width trials.
+
+    Mirrors gaffa's FfaPlan / FfaSearchPlan (include/gaffa/ffa_plan.h); the
+    width trials may be replaced as FfaSearchPlan::width_trials allows.
+    """
+
+    def __init__(self, tasks: np.ndarray, width_trials):
+        self.tasks = np.ascontiguousarray(tasks, _lib.TASK_DTYPE)
+        self.width_trials = tuple(int(w) for w in width_trials)
+
+    @property
+    def task_count(self) -> int:
+        return len(self.tasks)
+
+    @property
+    def nsamples(self) -> int:
+        return int(self.tasks[0]["input_nsamples"]) if len(self.tasks) else 0
+
+    def with_widths(self, widths) -> "FfaPlan":
+        return FfaPlan(self.tasks, widths)
+
+    def __repr__(self):
+        return f"FfaPlan(task_count={self.task_count}, width_trials={self.width_trials})"
+
+
+def make_riptide_ffa_plan(nsamples: int, tsamp: float, period_min: float, period_max: float,
+                          bins_min: int = 180, bins_max: int = 256, min_periods: int = 1,
+                          duty_cycle_max: float = 0.20, width_trial_spacing: float = 1.5,
+                          max_tasks: int = 1_000_000) -> FfaPlan:
+    """make_riptide_ffa_plan (src/gaffa/ffa_plan.cpp:90-170) via gf_make_riptide_ffa_plan."""
+    L = _lib.lib()
+    o = _lib.PlanOptions(period_min, period_max, bins_min, bins_max, min_periods, duty_cycle_max,
+                         width_trial_spacing, max_tasks)
+    nt, nw = _lib.u64(), _lib.u64()
+    check(L.gf_make_riptide_ffa_plan(nsamples, tsamp, C.byref(o), None, 0, C.byref(nt), None, 0, C.byref(nw)))
+    tasks = np.zeros(nt.value, _lib.TASK_DTYPE)
+    widths = np.zeros(nw.value, np.uint64)
+    check(L.gf_make_riptide_ffa_plan(nsamples, tsamp, C.byref(o), ptr(tasks), len(tasks), C.byref(nt),
+                                     ptr(widths), len(widths), C.byref(nw)))
+    return FfaPlan(tasks, widths)
+
+
+# ---------------------------------------------------------------------------
+# dedispersion
+# ---------------------------------------------------------------------------
+
+class DedispersionProgram:
+    """Delay tables and gather records for one observation geometry.
+
+    Counterpart of the host set-up inside dedisperse_*_cuda_device
+    (src/gaffa/dedispersion_cuda.cu:536-714).
+    """
+
+    def __init__(self, frequency_mhz, nsamples: int, tsamp: float, dm_low: float, dm_step: float,
+                 ndm: int, ref_frequency_mhz: float | None = None, chan_begin: int = 0,
+                 chan_end: int | None = None, nbits: int = 8, algorithm: str = "brute",
+                 subband_channels: int = 32, ndm_per_nominal: int = 32, device_id: int = 0):
+        self.device = _require_cuda(device_id)
+        self.device_id = device_id
+        self.freq = np.ascontiguousarray(frequency_mhz, np.float64)
+        nchans = len(self.freq)
+        self.nbits = nbits
+        self.nchans = nchans
+        self.nsamples = nsamples
+        self.ndm = ndm
+        self.algorithm = algorithm
+        self.ndm_per_nominal = ndm_per_nominal
+        fref = float(self.freq.max()) if ref_frequency_mhz is None else float(ref_frequency_mhz)
+        d = _lib.DedispDesc()
+        d.nsamples, d.nchans = nsamples, nchans
+        d.frequency_mhz = self.freq.ctypes.data_as(C.POINTER(C.c_double))
+        d.dm_low, d.dm_step, d.ndm = dm_low, dm_step, ndm
+        d.ref_frequency_mhz, d.tsamp = fref, tsamp
+        d.chan_begin = chan_begin
+        d.chan_end = nchans if chan_end is None else chan_end
+        d.nbits = nbits
+        d.algorithm = {"brute": _lib.DEDISP_BRUTE, "subband": _lib.DEDISP_SUBBAND}[algorithm]
+        d.subband_channels, d.ndm_per_nominal = subband_channels, ndm_per_nominal
+        d.device_id = device_id
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_dedisp_program_create(C.byref(d), C.byref(h)))
+        self._h = h
+        info = _lib.DedispInfo()
+        check(_lib.lib().gf_dedisp_program_info(h, C.byref(info)))
+        self.info = info
+        self.nout = int(info.nout)
+        self.dm_low, self.dm_step, self.tsamp = dm_low, dm_step, tsamp
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().gf_dedisp_program_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def row_bytes(self) -> int:
+        return self.nchans if self.nbits == 8 else self.nchans // 4
+
+    @property
+    def batch_granularity(self) -> int:
+        return 8 if self.algorithm == "brute" else self.ndm_per_nominal
+
+    def workspace_bytes(self, dm_count: int) -> int:
+        b = _lib.u64()
+        check(_lib.lib().gf_dedisp_workspace_bytes(self._h, dm_count, C.byref(b)))
+        return int(b.value)
+
+    def stage(self, data, stream=None) -> torch.Tensor:
+        """Channel-major staging of a time-major input (device tensor, or host
+        numpy array / tensor copied through a bounce buffer)."""
+        staged = torch.empty(int(self.info.staged_bytes), dtype=torch.uint8, device=self.device)
+        with torch.cuda.device(self.device):
+            if isinstance(data, torch.Tensor) and data.is_cuda:
+                if data.numel() * data.element_size() != self.info.input_bytes:
+                    raise ValueError("input size does not match the program geometry")
+                check(_lib.lib().gf_dedisp_stage(self._h, ptr(data), ptr(staged), _stream(stream)))
+            else:
+                host = data if isinstance(data, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(data))
+                if host.numel() * host.element_size() != self.info.input_bytes:
+                    raise ValueError("input size does not match the program geometry")
+                bounce_rows = max(128, (256 << 20) // self.row_bytes)
+                bounce = torch.empty(2 * bounce_rows * self.row_bytes, dtype=torch.uint8, device=self.device)
+                if not host.is_pinned():
+                    host = host.pin_memory()
+                check(_lib.lib().gf_dedisp_stage_from_host(self._h, ptr(host), ptr(staged), ptr(bounce),
+                                                           bounce.numel(), _stream(stream)))
+                torch.cuda.current_stream().synchronize()
+        return staged
+
+    def run(self, staged: torch.Tensor, dm_begin: int = 0, dm_count: int | None = None,
+            out: torch.Tensor | None = None, out_stride: int | None = None,
+            workspace: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """Dedisperse DMs [dm_begin, dm_begin + dm_count) into uint32
+        [dm_count][out_stride] (a view of `out` when given)."""
+        dm_count = self.ndm - dm_begin if dm_count is None else dm_count
+        out_stride = out_stride or ((self.nout + 3) // 4) * 4
+        if out is None:
+            out = torch.empty(dm_count * out_stride, dtype=torch.int32, device=self.device)
+        if self.algorithm == "subband" and workspace is None:
+            workspace = torch.empty(self.workspace_bytes(dm_count), dtype=torch.uint8, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_dedisp_run(self._h, ptr(staged), dm_begin, dm_count, ptr(out), out_stride,
+                                           ptr(workspace), _stream(stream)))
+        return out.view(-1)[: dm_count * out_stride].view(dm_count, out_stride)
+
+
+# ---------------------------------------------------------------------------
+# preprocessing
+# ---------------------------------------------------------------------------
+
+class PreprocessProgram:
+    """Riptide running-median detrend + normalise (CudaPreprocessProgram of
+    include/gaffa/preprocessing_cuda.h:44-89) for series of one length."""
+
+    def __init__(self, nsamples: int, tsamp: float, window_seconds: float = 5.0, min_points: int = 101,
+                 normalise: bool = True, reject_constant: bool = True, max_series: int = 16,
+                 device_id: int = 0):
+        self.device = _require_cuda(device_id)
+        self.desc = _lib.PreprocessDesc(tsamp, window_seconds, min_points, int(normalise),
+                                        int(reject_constant), nsamples, max_series)
+        self.info = _lib.PreprocessInfo()
+        check(_lib.lib().gf_preprocess_info_get(C.byref(self.desc), C.byref(self.info)))
+        self.workspace = torch.empty(max(16, int(self.info.workspace_bytes)), dtype=torch.uint8,
+                                     device=self.device)
+        self.stats = torch.zeros((max_series, 2), dtype=torch.float64, device=self.device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.nsamples = nsamples
+        self.max_series = max_series
+        self.normalise = normalise
+
+    def run(self, series: torch.Tensor, nseries: int | None = None, stream=None) -> torch.Tensor:
+        """In place on [nseries][stride] uint32 (int32 storage) or float32.
+        Returns the [nseries][2] FP64 (mean, 1/stddev) table."""
+        if series.dim() != 2:
+            raise ValueError("series must be [nseries][stride]")
+        nseries = series.shape[0] if nseries is None else nseries
+        is_u32 = series.dtype in (torch.int32, torch.uint32)
+        if not is_u32 and series.dtype != torch.float32:
+            raise TypeError("series must be uint32 (int32 storage) or float32")
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_preprocess_inplace(C.byref(self.desc), ptr(series), int(is_u32), nseries,
+                                                   series.stride(0), ptr(self.workspace), ptr(self.stats),
+                                                   ptr(self.status), _stream(stream)))
+        return self.stats[:nseries]
+
+    def synchronize(self) -> None:
+        """Waits and raises the deferred data error, as
+        CudaPreprocessProgram::synchronize (preprocessing_cuda.cu:781-817)."""
+        torch.cuda.current_stream(self.device).synchronize()
+        st = int(self.status.item())
+        self.status.zero_()
+        if st & _lib.STATUS_NONFINITE:
+            raise ValueError("running median detrend input samples must be finite")
+        if st & _lib.STATUS_CONSTANT:
+            raise ValueError("normalise input standard deviation must be finite and > 0")
+
+    def normalise_inplace(self, series: torch.Tensor, nseries: int, stream=None) -> None:
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_normalise(ptr(series), nseries, series.stride(0), self.nsamples,
+                                          ptr(self.stats), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# FFA
+# ---------------------------------------------------------------------------
+
+class FfaProgram:
+    """Device tables for one FFA plan (CudaFfaProgram,
+    src/gaffa/ffa_cuda_executor.cuh:44-80)."""
+
+    def __init__(self, plan: FfaPlan, max_series: int = 16, device_id: int = 0):
+        self.device = _require_cuda(device_id)
+        self.plan = plan
+        self.max_series = max_series
+        widths = np.ascontiguousarray(plan.width_trials, np.uint64)
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_ffa_program_create(ptr(plan.tasks), len(plan.tasks), ptr(widths), len(widths),
+                                                   max_series, device_id, C.byref(h)))
+        self._h = h
+        self.info = _lib.FfaInfo()
+        check(_lib.lib().gf_ffa_program_info(h, C.byref(self.info)))
+        self.scratch = torch.empty(max(16, int(self.info.scratch_bytes)), dtype=torch.uint8, device=self.device)
+        self.counters = torch.zeros(2, dtype=torch.int64, device=self.device)
+        self.capacity = 1 << 16
+        self.peaks = torch.empty(self.capacity * 24, dtype=torch.uint8, device=self.device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().gf_ffa_program_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def prepared_floats(self) -> int:
+        return int(self.info.prepared_floats)
+
+    def prepare(self, series: torch.Tensor, nseries: int, stats: torch.Tensor | None = None,
+                out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty((nseries, self.prepared_floats), dtype=torch.float32, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_ffa_prepare(self._h, ptr(series), nseries, series.stride(0), ptr(stats), ptr(out),
+                                            _stream(stream)))
+        return out
+
+    def search_async(self, prepared: torch.Tensor, nseries: int, snr_threshold: float, stream=None):
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_ffa_search(self._h, ptr(prepared), nseries, snr_threshold, ptr(self.scratch),
+                                           ptr(self.peaks), self.capacity, ptr(self.counters), _stream(stream)))
+
+    def search(self, prepared: torch.Tensor, nseries: int, snr_threshold: float = 6.0,
+               max_peaks: int = 0, stream=None) -> np.ndarray:
+        """Transform + detect every task of every series; returns the compact
+        peak records (PEAK_RECORD_DTYPE, unordered).  A peak buffer overflow
+        grows the buffer and re-runs, as CudaFfaTileRunner does
+        (ffa_cuda_executor.cuh:395-404,491-531)."""
+        if not math.isfinite(snr_threshold):
+            raise ValueError("FFA search S/N threshold must be finite")
+        while True:
+            self.search_async(prepared, nseries, snr_threshold, stream)
+            counts = self.counters.cpu()
+            n = int(counts[0])
+            if n <= self.capacity:
+                break
+            self.capacity = int(n * 1.25) + 1024
+            self.peaks = torch.empty(self.capacity * 24, dtype=torch.uint8, device=self.device)
+        if max_peaks and n > max_peaks * nseries:
+            raise RuntimeError("FFA detection peak count exceeded max_peaks safety guard")
+        raw = self.peaks[: n * 24].cpu().numpy()
+        return raw.view(_lib.PEAK_RECORD_DTYPE).copy()
+
+    def expand(self, records: np.ndarray, series_offset: int = 0, dm_low: float = 0.0,
+               dm_step: float = 0.0) -> np.ndarray:
+        records = np.ascontiguousarray(records, _lib.PEAK_RECORD_DTYPE)
+        out = np.zeros(len(records), _lib.PEAK_DTYPE)
+        check(_lib.lib().gf_ffa_expand_peaks(self._h, ptr(records), len(records), series_offset, dm_low, dm_step,
+                                             ptr(out)))
+        return out
+
+
+def ffa_transform(x: torch.Tensor, bins: int, stream=None) -> torch.Tensor:
+    """Materialised FFA transform of the first rows*bins samples (ffa_transform_cpu,
+    src/gaffa/ffa.cpp:389-417) on the device."""
+    rows = x.numel() // bins
+    out = torch.empty((rows, bins), dtype=torch.float32, device=x.device)
+    scratch = torch.empty(2 * rows * bins, dtype=torch.float32, device=x.device)
+    src = x.reshape(-1)[: rows * bins].contiguous()
+    with torch.cuda.device(x.device):
+        check(_lib.lib().gf_ffa_transform(ptr(src), rows, bins, ptr(out), ptr(scratch), _stream(stream)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# host post-processing
+# ---------------------------------------------------------------------------
+
+def sort_peaks(peaks: np.ndarray) -> np.ndarray:
+    peaks = np.ascontiguousarray(peaks, _lib.PEAK_DTYPE).copy()
+    check(_lib.lib().gf_sort_peaks(ptr(peaks), len(peaks)))
+    return peaks
+
+
+def select_candidates(peaks: np.ndarray, observation_seconds: float, frequency_cluster_radius: float = 0.1,
+                      dm_cluster_radius: int = 1, cluster_across_widths: bool = True,
+                      max_candidates: int = 0) -> np.ndarray:
+    """select_candidates_cpu (src/gaffa/candidate.cpp:175-212)."""
+    peaks = np.ascontiguousarray(peaks, _lib.PEAK_DTYPE)
+    o = _lib.CandidateOptions(frequency_cluster_radius, dm_cluster_radius, int(cluster_across_widths), 0,
+                              max_candidates)
+    n = _lib.u64()
+    check(_lib.lib().gf_select_candidates(ptr(peaks), len(peaks), observation_seconds, C.byref(o), None, 0,
+                                          C.byref(n)))
+    out = np.zeros(n.value, _lib.CAND_DTYPE)
+    check(_lib.lib().gf_select_candidates(ptr(peaks), len(peaks), observation_seconds, C.byref(o), ptr(out),
+                                          len(out), C.byref(n)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# folding
+# ---------------------------------------------------------------------------
+
+def fold_time_series(series: torch.Tensor, period: float, tsamp: float, nbin: int, start_sample: int = 0,
+                     stream=None):
+    """fold_time_series_cpu (src/gaffa/folding.cpp:452-502) on a device series
+    (uint32 stored as int32, or float32).  Returns host (profile, exposure)."""
+    if series.dim() != 1:
+        series = series.reshape(-1)
+    is_u32 = series.dtype in (torch.int32, torch.uint32)
+    n = series.numel()
+    ws_bytes = int(_lib.lib().gf_fold_workspace_bytes(n, nbin))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=series.device)
+    prof = torch.empty(nbin, dtype=torch.float32, device=series.device)
+    expo = torch.empty(nbin, dtype=torch.float64, device=series.device)
+    with torch.cuda.device(series.device):
+        check(_lib.lib().gf_fold_time_series(ptr(series), int(is_u32), n, period, tsamp, nbin, start_sample,
+                                             ptr(prof), ptr(expo), ptr(ws), _stream(stream)))
+    status = int(ws[ws_bytes - 16: ws_bytes - 12].view(torch.int32).item())
+    if status & _lib.STATUS_NONFINITE:
+        raise ValueError("fold input must contain only finite samples")
+    return prof.cpu().numpy(), expo.cpu().numpy()
+
+
+# ---------------------------------------------------------------------------
+# synthetic observations
+# ---------------------------------------------------------------------------
+
+def synth_generate(obs, t_begin: int = 0, t_end: int | None = None, out: torch.Tensor | None = None,
+                   device_id: int = 0, stream=None) -> torch.Tensor:
+    """The synth.py observation generated on the device (same noise bits)."""
+    from . import synth
+    device = _require_cuda(device_id)
+    t_end = obs.nsamples if t_end is None else t_end
+    row = obs.nchans if obs.nbits == 8 else obs.nchans // 4
+    if out is None:
+        out = torch.empty((t_end - t_begin, row), dtype=torch.uint8, device=device)
+    ps = (_lib.SynthPulsar * max(1, len(obs.pulsars)))()
+    for i, p in enumerate(obs.pulsars):
+        ps[i] = _lib.SynthPulsar(p.period, p.dm, p.duty_cycle, p.amplitude, p.phase)
+    d = _lib.SynthDesc()
+    d.nchans, d.nsamples, d.tsamp = obs.nchans, obs.nsamples, obs.tsamp
+    d.f_low, d.f_high, d.nbits = obs.f_low, obs.f_high, obs.nbits
+    d.npulsars, d.seed = len(obs.pulsars), obs.seed
+    d.pulsars = C.cast(ps, C.POINTER(_lib.SynthPulsar))
+    r = obs.rfi
+    d.narrowband_fraction, d.narrowband_hz, d.narrowband_amplitude = (r.narrowband_fraction, r.narrowband_hz,
+                                                                      r.narrowband_amplitude)
+    d.impulse_hz, d.impulse_amplitude = r.impulse_hz, r.impulse_amplitude
+    mask = None
+    if r.narrowband_fraction > 0.0:
+        mask = np.ascontiguousarray(synth._narrowband_mask(obs).astype(np.uint8))
+        d.narrowband_mask = mask.ctypes.data_as(C.POINTER(C.c_uint8))
+    with torch.cuda.device(device):
+        check(_lib.lib().gf_synth_generate(C.byref(d), t_begin, t_end, ptr(out), _stream(stream)))
+    return out

@@ -1,0 +1,777 @@
+// Brute-force and subband incoherent dedispersion for sm_100a.
+//
+// Reference arithmetic: dedispersion.cpp:197-215 (direct_sum_at),
+// :291-329 (dedisperse_multi_dm_cpu), :331-453 (dedisperse_subband_cpu) and
+// internal/dedispersion_delay.h:37-139 (delay tables).  Sums are integer, so
+// any summation order is bit-exact.
+//
+// Layout.  The time-major input ([time][chan] uint8, or packed 2-bit) is
+// staged once into channel-major rows (one uint8 row per channel, row stride
+// a multiple of 16 bytes); every DM block reuses it.
+//
+// Kernel.  One CTA = a block of DB DMs x a time tile; each warp owns one DM and
+// 1008 consecutive output samples (252 output words of 4 samples).  The CTA
+// streams channel chunks: for each channel it copies the window
+// [t0 + base, t0 + base + RS) (base = delay of the block's first DM rounded down
+// to 16) into shared memory with 16-byte loads.  A warp reads its DM's shifted
+// window as aligned 32-bit words: the delay offset off = d - base splits into a
+// word offset q = off >> 2 and a byte class s = off & 3.  The host sorts each
+// warp's channels by class, so the class is static inside the loop: a word
+// holds 4 consecutive input bytes, which are split into even/odd byte pairs
+// (LOP3 and PRMT) and accumulated in 16-bit lanes (IADD3 folds two channels).
+// Per 256 channels the 16-bit lanes are flushed into 32-bit sums, realigning
+// class s by s bytes with one lane shuffle.  Lanes read consecutive words, so
+// every LDS.32 is conflict-free.
+#include "common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <vector>
+
+namespace gf {
+
+int32_t delay_bins(double dm, double f, double fref, double tsamp) {
+  const double f2 = f * f;
+  const double ref2 = fref * fref;
+  const double delay = 4148.808 * dm * (1.0 / f2 - 1.0 / ref2);
+  const double bins = std::round(delay / tsamp);
+  if (bins < static_cast<double>(std::numeric_limits<int32_t>::min()) ||
+      bins > static_cast<double>(std::numeric_limits<int32_t>::max()))
+    raise(GF_EOVERFLOW, "dedispersion delay exceeds int32 range");
+  return static_cast<int32_t>(bins);
+}
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kWords = 8;                       // input words per lane
+constexpr int kOutWords = 32 * kWords - 4;      // 252 output words per warp
+constexpr int kWarpSamples = 4 * kOutWords;     // 1008 samples per warp
+constexpr int kFlushChannels = 256;             // 16-bit lanes hold 256 x 255
+constexpr unsigned kFull = 0xffffffffu;
+
+struct BytesParams {
+  const uint8_t* in;         // group 0, row 0 of the launch
+  uint64_t in_row_stride;    // bytes between channel rows
+  uint64_t in_group_stride;  // bytes between groups
+  uint64_t in_valid;         // valid samples per row (zero beyond)
+  int rows_per_group;
+  int total_rows;            // group g has min(rows_per_group, total_rows - g*rows_per_group) rows
+  const int32_t* base;       // + g*base_group_stride + blockIdx.y*rows_per_group
+  uint64_t base_group_stride;
+  const uint32_t* records;   // + g*rec_group_stride + dm*rec_dm_stride + chunk*record_words
+  uint64_t rec_group_stride;
+  uint64_t rec_dm_stride;
+  int dm_count;              // DMs per group handled by the launch
+  int dm_count_last;         // DMs of the launch's last group
+  int ngroups;
+  int dms_per_cta;
+  int warps_per_dm;
+  int chunk_rows;
+  int nchunks;
+  int row_bytes;
+  int record_words;
+  uint64_t cta_samples;
+  void* out;                 // row (dm*out_dm_rows + g*out_group_rows)
+  uint64_t out_row_stride;   // elements between output rows
+  uint64_t out_dm_rows;
+  uint64_t out_group_rows;
+  uint64_t nout;             // valid output samples
+};
+
+__device__ __forceinline__ uint32_t lo16(uint32_t v) { return v & 0xffffu; }
+__device__ __forceinline__ uint32_t hi16(uint32_t v) { return v >> 16; }
+// byte position b (0..3) of the 4-sample word, from the even/odd accumulators
+__device__ __forceinline__ uint32_t pos_sum(uint32_t e, uint32_t o, int b) {
+  return b == 0 ? lo16(e) : b == 1 ? lo16(o) : b == 2 ? hi16(e) : hi16(o);
+}
+
+template <int S>
+__device__ __forceinline__ void flush_class(uint32_t (&e)[kWords], uint32_t (&o)[kWords],
+                                            uint32_t (&out)[kWords][4], int lane) {
+#pragma unroll
+  for (int m = 0; m < kWords; ++m) {
+    if (S == 0) {
+#pragma unroll
+      for (int p = 0; p < 4; ++p) out[m][p] += pos_sum(e[m], o[m], p);
+    } else {
+      // class S word j contributes to output positions p = b - S of word j
+      // (b >= S) and p = b - S + 4 of word j - 1 (b < S); so output word j
+      // takes bytes b >= S of word j and bytes b < S of word j + 1.
+      uint32_t ne = __shfl_down_sync(kFull, e[m], 1);
+      uint32_t no = __shfl_down_sync(kFull, o[m], 1);
+      const uint32_t we = __shfl_sync(kFull, m + 1 < kWords ? e[(m + 1) % kWords] : 0u, 0);
+      const uint32_t wo = __shfl_sync(kFull, m + 1 < kWords ? o[(m + 1) % kWords] : 0u, 0);
+      if (lane == 31) { ne = we; no = wo; }
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const int b = p + S;
+        out[m][p] += b < 4 ? pos_sum(e[m], o[m], b) : pos_sum(ne, no, b - 4);
+      }
+    }
+    e[m] = 0u;
+    o[m] = 0u;
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void accumulate_class(const uint32_t* __restrict__ smem_words,
+                                                 const uint32_t* __restrict__ rec, int& pos,
+                                                 int npairs, int lane_word,
+                                                 uint32_t (&e)[kWords], uint32_t (&o)[kWords]) {
+  for (int i = 0; i < npairs; ++i) {
+    const uint32_t entry = rec[pos + i];
+    const uint32_t* a = smem_words + (entry & 0xffffu) + lane_word;
+    const uint32_t* b = smem_words + (entry >> 16) + lane_word;
+#pragma unroll
+    for (int m = 0; m < kWords; ++m) {
+      const uint32_t w1 = a[32 * m];
+      const uint32_t w2 = b[32 * m];
+      e[m] += (w1 & 0x00ff00ffu) + (w2 & 0x00ff00ffu);
+      o[m] += __byte_perm(w1, 0u, 0x4341) + __byte_perm(w2, 0u, 0x4341);
+    }
+  }
+  pos += npairs;
+}
+
+template <typename OutT>
+__global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesParams p) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int group = blockIdx.z;
+  const int block = blockIdx.y;
+  const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * p.cta_samples;
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int dm_sub = warp / p.warps_per_dm;
+  const int sub = warp % p.warps_per_dm;
+  const int dm_local = block * p.dms_per_cta + dm_sub;
+  const int dm_limit = group + 1 == p.ngroups ? p.dm_count_last : p.dm_count;
+  const bool active = dm_sub < p.dms_per_cta && dm_local < dm_limit;
+
+  const int group_rows = min(p.rows_per_group, p.total_rows - group * p.rows_per_group);
+  uint8_t* rows = smem;
+  uint32_t* rec_smem = reinterpret_cast<uint32_t*>(smem + (p.chunk_rows + 1) * p.row_bytes);
+  const uint32_t* smem_words = reinterpret_cast<const uint32_t*>(smem);
+  const uint8_t* in_group = p.in + group * p.in_group_stride;
+  const int32_t* base = p.base + group * p.base_group_stride + static_cast<uint64_t>(block) * p.rows_per_group;
+
+  // zero row (index chunk_rows) for class padding entries
+  for (int i = threadIdx.x; i < p.row_bytes / 16; i += kThreads)
+    reinterpret_cast<uint4*>(rows + p.chunk_rows * p.row_bytes)[i] = make_uint4(0, 0, 0, 0);
+
+  uint32_t e[4][kWords], o[4][kWords], acc[kWords][4];
+#pragma unroll
+  for (int m = 0; m < kWords; ++m) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) { e[s][m] = 0u; o[s][m] = 0u; }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[m][q] = 0u;
+  }
+  const int lane_word = sub * kOutWords + lane;
+  const int chunks_per_flush = kFlushChannels / p.chunk_rows;
+
+  for (int k = 0; k < p.nchunks; ++k) {
+    const int row0 = k * p.chunk_rows;
+    const int nrows = min(p.chunk_rows, group_rows - row0);
+    __syncthreads();
+    // stage the chunk's channel windows
+    const int vecs_per_row = p.row_bytes / 16;
+    for (int i = threadIdx.x; i < nrows * vecs_per_row; i += kThreads) {
+      const int r = i / vecs_per_row;
+      const int v = i - r * vecs_per_row;
+      const uint64_t t = t0 + static_cast<uint64_t>(base[row0 + r]) + 16ull * v;
+      const uint8_t* src = in_group + static_cast<uint64_t>(row0 + r) * p.in_row_stride + t;
+      uint4 val;
+      if (t + 16 <= p.in_valid) {
+        val = __ldg(reinterpret_cast<const uint4*>(src));
+      } else {
+        uint8_t tmp[16];
+#pragma unroll
+        for (int b = 0; b < 16; ++b) tmp[b] = (t + b < p.in_valid) ? src[b] : 0;
+        memcpy(&val, tmp, 16);
+      }
+      reinterpret_cast<uint4*>(rows + r * p.row_bytes)[v] = val;
+    }
+    for (int i = threadIdx.x; i < p.dms_per_cta * p.record_words; i += kThreads) {
+      const int d = i / p.record_words;
+      const int w = i - d * p.record_words;
+      const int dl = block * p.dms_per_cta + d;
+      uint32_t val = 0u;
+      if (dl < dm_limit)
+        val = p.records[group * p.rec_group_stride + dl * p.rec_dm_stride +
+                        static_cast<uint64_t>(k) * p.record_words + w];
+      rec_smem[i] = val;
+    }
+    __syncthreads();
+    if (active) {
+      const uint32_t* rec = rec_smem + dm_sub * p.record_words;
+      const uint32_t counts = rec[0];
+      int pos = 1;
+      accumulate_class<0>(smem_words, rec, pos, (counts & 0xffu) >> 1, lane_word, e[0], o[0]);
+      accumulate_class<1>(smem_words, rec, pos, ((counts >> 8) & 0xffu) >> 1, lane_word, e[1], o[1]);
+      accumulate_class<2>(smem_words, rec, pos, ((counts >> 16) & 0xffu) >> 1, lane_word, e[2], o[2]);
+      accumulate_class<3>(smem_words, rec, pos, (counts >> 24) >> 1, lane_word, e[3], o[3]);
+      if ((k + 1) % chunks_per_flush == 0 || k + 1 == p.nchunks) {
+        flush_class<0>(e[0], o[0], acc, lane);
+        flush_class<1>(e[1], o[1], acc, lane);
+        flush_class<2>(e[2], o[2], acc, lane);
+        flush_class<3>(e[3], o[3], acc, lane);
+      }
+    }
+  }
+  if (!active) return;
+  OutT* out = static_cast<OutT*>(p.out) +
+              (static_cast<uint64_t>(dm_local) * p.out_dm_rows +
+               static_cast<uint64_t>(group) * p.out_group_rows) * p.out_row_stride;
+#pragma unroll
+  for (int m = 0; m < kWords; ++m) {
+    const int j = lane + 32 * m;
+    if (j >= kOutWords) continue;
+    const uint64_t t = t0 + static_cast<uint64_t>(sub) * kWarpSamples + 4ull * j;
+    if (t >= p.nout) continue;
+    if (sizeof(OutT) == 4 && t + 4 <= p.nout && (p.out_row_stride & 3) == 0) {
+      *reinterpret_cast<uint4*>(out + t) = make_uint4(acc[m][0], acc[m][1], acc[m][2], acc[m][3]);
+    } else if (sizeof(OutT) == 1 && t + 4 <= p.nout && (p.out_row_stride & 3) == 0) {
+      *reinterpret_cast<uint32_t*>(out + t) =
+          acc[m][0] | (acc[m][1] << 8) | (acc[m][2] << 16) | (acc[m][3] << 24);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (t + q < p.nout) out[t + q] = static_cast<OutT>(acc[m][q]);
+    }
+  }
+}
+
+// Stage-2 sum over uint32 intermediate rows (subband with 8-bit input, where
+// partial sums exceed a byte): out[dm][t] = sum_b inter[b][t + r(dm, b)].
+__global__ void __launch_bounds__(256) subband_stage2_u32_kernel(
+    const uint32_t* __restrict__ inter, uint64_t inter_row_stride, uint64_t inter_group_stride,
+    uint64_t inter_valid, int nsb, const int32_t* __restrict__ resid, int ndm_group,
+    uint32_t* __restrict__ out, uint64_t out_row_stride, uint64_t nout) {
+  const int group = blockIdx.z;
+  const int dm_local = blockIdx.y;
+  if (dm_local >= ndm_group) return;
+  const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nout) return;
+  const uint32_t* base = inter + group * inter_group_stride;
+  const int32_t* r = resid + (static_cast<uint64_t>(group) * ndm_group + dm_local) * nsb;
+  uint32_t sum = 0;
+  for (int b = 0; b < nsb; ++b) {
+    const uint64_t st = t + static_cast<uint64_t>(r[b]);
+    if (st < inter_valid) sum += __ldg(base + b * inter_row_stride + st);
+  }
+  out[(static_cast<uint64_t>(group) * ndm_group + dm_local) * out_row_stride + t] = sum;
+}
+
+// Time-major [nsamples][row_bytes] -> channel-major rows [chan][row_stride]
+// for channels [chan_begin, chan_end); 8-bit copy or 2-bit unpack (channel
+// 4k+j in bits [2j, 2j+1] of byte k).  64 samples x 64 channels per CTA.
+template <int Bits>
+__global__ void __launch_bounds__(256) stage_kernel(const uint8_t* __restrict__ in, uint64_t nsamples,
+                                                    uint64_t in_row_bytes, int chan_begin, int nchan,
+                                                    uint8_t* __restrict__ out, uint64_t out_stride,
+                                                    uint64_t t_offset) {
+  __shared__ uint8_t tile[64][64 + 4];
+  const uint64_t tb = static_cast<uint64_t>(blockIdx.x) * 64;
+  const int cb = blockIdx.y * 64;
+  for (int i = threadIdx.x; i < 64 * 64; i += 256) {
+    const int tt = i / 64, cc = i % 64;
+    const uint64_t t = tb + tt;
+    const int c = cb + cc;
+    uint8_t v = 0;
+    if (t < nsamples && c < nchan) {
+      const int ch = chan_begin + c;
+      if (Bits == 8) {
+        v = in[t * in_row_bytes + ch];
+      } else {
+        v = (in[t * in_row_bytes + (ch >> 2)] >> (2 * (ch & 3))) & 3u;
+      }
+    }
+    tile[tt][cc] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 64 * 64; i += 256) {
+    const int cc = i / 64, tt = i % 64;
+    const uint64_t t = tb + tt;
+    const int c = cb + cc;
+    if (t < nsamples && c < nchan) out[static_cast<uint64_t>(c) * out_stride + t_offset + t] = tile[tt][cc];
+  }
+}
+
+// Class-sorted gather records: word 0 packs the four (even) class counts,
+// then (chunk_rows + 4) / 2 words of u16 entry pairs.
+struct Records {
+  std::vector<uint32_t> words;
+  std::vector<int32_t> base;
+  int record_words = 0;
+  int nchunks = 0;
+  int max_off = 0;
+};
+
+// delays: [ngroups][ndm_group][rows_per_group] (rows beyond a ragged last
+// group are ignored).  Builds base[group][block][row] and the records.
+Records build_records(const std::vector<int32_t>& delays, int ngroups, int ndm_group,
+                      int rows_per_group, int total_rows, int dms_per_cta, int chunk_rows,
+                      int row_bytes) {
+  Records r;
+  const int blocks = static_cast<int>(ceil_div(ndm_group, dms_per_cta));
+  r.nchunks = static_cast<int>(ceil_div(rows_per_group, chunk_rows));
+  r.record_words = static_cast<int>(round_up(1 + (chunk_rows + 4) / 2, 4));
+  r.base.assign(static_cast<size_t>(ngroups) * blocks * rows_per_group, 0);
+  r.words.assign(static_cast<size_t>(ngroups) * ndm_group * r.nchunks * r.record_words, 0u);
+  const int zero_word = chunk_rows * row_bytes / 4;
+  std::vector<uint16_t> cls[4];
+  for (int g = 0; g < ngroups; ++g) {
+    const int grows = std::min(rows_per_group, total_rows - g * rows_per_group);
+    for (int b = 0; b < blocks; ++b) {
+      const int d0 = b * dms_per_cta;
+      for (int row = 0; row < grows; ++row) {
+        const int32_t d = delays[(static_cast<size_t>(g) * ndm_group + d0) * rows_per_group + row];
+        r.base[(static_cast<size_t>(g) * blocks + b) * rows_per_group + row] = d & ~15;
+      }
+    }
+    for (int dm = 0; dm < ndm_group; ++dm) {
+      const int b = dm / dms_per_cta;
+      for (int k = 0; k < r.nchunks; ++k) {
+        for (auto& c : cls) c.clear();
+        const int row0 = k * chunk_rows;
+        const int nrows = std::min(chunk_rows, grows - row0);
+        for (int i = 0; i < nrows; ++i) {
+          const int row = row0 + i;
+          const int32_t d = delays[(static_cast<size_t>(g) * ndm_group + dm) * rows_per_group + row];
+          const int32_t off = d - r.base[(static_cast<size_t>(g) * blocks + b) * rows_per_group + row];
+          r.max_off = std::max(r.max_off, off);
+          const int word = i * (row_bytes / 4) + (off >> 2);
+          cls[off & 3].push_back(static_cast<uint16_t>(word));
+        }
+        uint32_t* rec = r.words.data() +
+                        ((static_cast<size_t>(g) * ndm_group + dm) * r.nchunks + k) * r.record_words;
+        uint32_t counts = 0;
+        std::vector<uint16_t> flat;
+        for (int s = 0; s < 4; ++s) {
+          if (cls[s].size() & 1) cls[s].push_back(static_cast<uint16_t>(zero_word));
+          counts |= static_cast<uint32_t>(cls[s].size()) << (8 * s);
+          flat.insert(flat.end(), cls[s].begin(), cls[s].end());
+        }
+        rec[0] = counts;
+        for (size_t i = 0; i + 1 < flat.size(); i += 2)
+          rec[1 + i / 2] = static_cast<uint32_t>(flat[i]) | (static_cast<uint32_t>(flat[i + 1]) << 16);
+      }
+    }
+  }
+  return r;
+}
+
+struct Launch {
+  int dms_per_cta = kWarps;
+  int warps_per_dm = 1;
+  int chunk_rows = 64;
+  int row_bytes = 0;
+  size_t smem = 0;
+};
+
+// Picks the DM block size and channel chunk so the staged windows fit in
+// shared memory with two CTAs per SM when possible.
+template <typename F>
+Launch choose_launch(F&& max_off_for) {
+  const size_t budget2 = 110 * 1024, budget1 = 220 * 1024;
+  for (size_t budget : {budget2, budget1}) {
+    for (int dpc : {8, 4, 2, 1}) {
+      const int wpd = kWarps / dpc;
+      const int max_off = max_off_for(dpc);
+      const int row_bytes = static_cast<int>(round_up(max_off + 4 * ((wpd - 1) * kOutWords + 32 * kWords), 16));
+      for (int cr : {64, 32, 16, 8}) {
+        const size_t rec = static_cast<size_t>(dpc) * round_up(1 + (cr + 4) / 2, 4) * 4;
+        const size_t smem = static_cast<size_t>(cr + 1) * row_bytes + rec;
+        if (smem <= budget && static_cast<size_t>(cr + 1) * row_bytes < 262144) {
+          return Launch{dpc, wpd, cr, row_bytes, smem};
+        }
+      }
+    }
+  }
+  raise(GF_EINVAL, "dedispersion delay spread too large for a shared-memory tile");
+}
+
+int max_off_estimate(const std::vector<int32_t>& delays, int ngroups, int ndm_group,
+                     int rows_per_group, int total_rows, int dpc) {
+  int mo = 0;
+  for (int g = 0; g < ngroups; ++g) {
+    const int grows = std::min(rows_per_group, total_rows - g * rows_per_group);
+    for (int dm = 0; dm < ndm_group; ++dm) {
+      const int d0 = (dm / dpc) * dpc;
+      for (int row = 0; row < grows; ++row) {
+        const int32_t d = delays[(static_cast<size_t>(g) * ndm_group + dm) * rows_per_group + row];
+        const int32_t b = delays[(static_cast<size_t>(g) * ndm_group + d0) * rows_per_group + row] & ~15;
+        mo = std::max(mo, d - b);
+      }
+    }
+  }
+  return mo;
+}
+
+// One bytes-kernel configuration with its device tables: ngroups groups of
+// ndm_group DMs over rows_per_group rows (ragged last group).
+struct BytesStage {
+  Launch launch;
+  Records rec;
+  DeviceBlob base_dev, rec_dev;
+  int ngroups = 0, ndm_group = 0, rows_per_group = 0, total_rows = 0, blocks = 0;
+
+  void build(const std::vector<int32_t>& delays, int ng, int ndg, int rpg, int tr, int device) {
+    ngroups = ng;
+    ndm_group = ndg;
+    rows_per_group = rpg;
+    total_rows = tr;
+    launch = choose_launch([&](int dpc) { return max_off_estimate(delays, ng, ndg, rpg, tr, dpc); });
+    blocks = static_cast<int>(ceil_div(ndg, launch.dms_per_cta));
+    rec = build_records(delays, ng, ndg, rpg, tr, launch.dms_per_cta, launch.chunk_rows, launch.row_bytes);
+    base_dev.upload(rec.base.data(), rec.base.size() * sizeof(int32_t), device);
+    rec_dev.upload(rec.words.data(), rec.words.size() * sizeof(uint32_t), device);
+  }
+
+  uint64_t metadata_bytes() const { return base_dev.bytes + rec_dev.bytes; }
+
+  // Launch for groups [g0, g0 + gcount) and, within each group, DMs
+  // [dm_first, dm_first + dm_count) (dm_first a multiple of the DM block);
+  // the last launched group handles dm_count_last DMs.  in / out point at the
+  // launch's first group and first output row.
+  template <typename OutT>
+  void run(const uint8_t* in, uint64_t row_stride, uint64_t group_stride, uint64_t valid, int g0,
+           int gcount, int dm_first, int dm_count, int dm_count_last, void* out,
+           uint64_t out_row_stride, uint64_t out_dm_rows, uint64_t out_group_rows, uint64_t nout,
+           cudaStream_t stream) const {
+    if (dm_first % launch.dms_per_cta != 0) raise(GF_EINVAL, "DM range not aligned to the DM block");
+    BytesParams p{};
+    p.in = in;
+    p.in_row_stride = row_stride;
+    p.in_group_stride = group_stride;
+    p.in_valid = valid;
+    p.rows_per_group = rows_per_group;
+    p.total_rows = total_rows - g0 * rows_per_group;
+    p.base_group_stride = static_cast<uint64_t>(blocks) * rows_per_group;
+    p.base = base_dev.as<int32_t>() + g0 * p.base_group_stride +
+             static_cast<uint64_t>(dm_first / launch.dms_per_cta) * rows_per_group;
+    p.rec_dm_stride = static_cast<uint64_t>(rec.nchunks) * rec.record_words;
+    p.rec_group_stride = static_cast<uint64_t>(ndm_group) * p.rec_dm_stride;
+    p.records = rec_dev.as<uint32_t>() + g0 * p.rec_group_stride + dm_first * p.rec_dm_stride;
+    p.dm_count = dm_count;
+    p.dm_count_last = dm_count_last;
+    p.ngroups = gcount;
+    p.dms_per_cta = launch.dms_per_cta;
+    p.warps_per_dm = launch.warps_per_dm;
+    p.chunk_rows = launch.chunk_rows;
+    p.nchunks = rec.nchunks;
+    p.row_bytes = launch.row_bytes;
+    p.record_words = rec.record_words;
+    p.cta_samples = static_cast<uint64_t>(launch.warps_per_dm) * kWarpSamples;
+    p.out = out;
+    p.out_row_stride = out_row_stride;
+    p.out_dm_rows = out_dm_rows;
+    p.out_group_rows = out_group_rows;
+    p.nout = nout;
+    const int dmax = std::max(dm_count, dm_count_last);
+    dim3 grid(static_cast<unsigned>(ceil_div(nout, p.cta_samples)),
+              static_cast<unsigned>(ceil_div(dmax, launch.dms_per_cta)), static_cast<unsigned>(gcount));
+    auto kernel = dedisperse_bytes_kernel<OutT>;
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(launch.smem)),
+               "cudaFuncSetAttribute(dedisperse smem)");
+    kernel<<<grid, kThreads, launch.smem, stream>>>(p);
+    cuda_check(cudaGetLastError(), "dedisperse_bytes_kernel launch");
+  }
+};
+
+}  // namespace
+}  // namespace gf
+
+using namespace gf;
+
+struct gf_dedisp_program {
+  gf_dedisp_desc desc{};
+  std::vector<double> freq;
+  uint64_t nc = 0;          // selected channels
+  uint64_t nout = 0;
+  int32_t max_delay = 0;
+  uint64_t row_stride = 0;  // staged bytes per channel row
+  // brute force
+  BytesStage brute;
+  // subband
+  uint64_t nsb = 0, sbc = 0, nnom = 0, npn = 0;
+  uint64_t inter_len = 0, inter_row_stride = 0;
+  bool inter_u8 = false;
+  BytesStage stage1, stage2;
+  std::vector<int32_t> resid;
+  DeviceBlob resid_dev;
+};
+
+namespace {
+
+void validate_desc(const gf_dedisp_desc& d) {
+  // dedispersion.cpp:49-139 validation order
+  check_arg(d.nsamples > 0, "dedispersion requires at least one sample");
+  check_arg(d.nchans > 0, "dedispersion requires at least one channel");
+  check_arg(d.frequency_mhz != nullptr, "frequency table must not be null");
+  for (uint64_t c = 0; c < d.nchans; ++c)
+    check_arg(std::isfinite(d.frequency_mhz[c]) && d.frequency_mhz[c] > 0.0,
+              "frequency values must be finite and positive");
+  check_arg(std::isfinite(d.ref_frequency_mhz) && d.ref_frequency_mhz > 0.0,
+            "reference frequency must be positive");
+  check_arg(std::isfinite(d.tsamp) && d.tsamp > 0.0, "tsamp must be positive");
+  check_arg(std::isfinite(d.dm_low) && d.dm_low >= 0.0, "dm_low must be finite and non-negative");
+  check_arg(d.ndm > 0, "dedispersion requires at least one DM");
+  check_arg(std::isfinite(d.dm_step) && d.dm_step > 0.0, "dm_step must be positive");
+  check_arg(d.chan_begin < d.chan_end, "channel range must be non-empty");
+  check_arg(d.chan_end <= d.nchans, "channel range exceeds sample channel count");
+  for (uint64_t c = d.chan_begin; c < d.chan_end; ++c)
+    check_arg(d.frequency_mhz[c] <= d.ref_frequency_mhz,
+              "dedispersion requires selected frequencies <= reference frequency");
+  check_arg(d.nbits == 8 || d.nbits == 2, "nbits must be 8 or 2");
+  check_arg(d.nbits != 2 || d.nchans % 4 == 0, "2-bit input requires nchans % 4 == 0");
+  check_arg(d.algorithm == GF_DEDISP_BRUTE || d.algorithm == GF_DEDISP_SUBBAND,
+            "unknown dedispersion algorithm");
+  if (d.algorithm == GF_DEDISP_SUBBAND) {
+    check_arg(d.subband_channels > 0, "subband_channels must be positive");
+    check_arg(d.ndm_per_nominal > 0, "ndm_per_nominal must be positive");
+  }
+  check_arg(d.chan_end - d.chan_begin < 65536, "at most 65535 channels per program");
+  check_arg(d.ndm < (1ull << 31), "too many DM trials");
+}
+
+}  // namespace
+
+extern "C" int gf_dedisp_program_create(const gf_dedisp_desc* desc, gf_dedisp_program** out) {
+  return guarded([&] {
+    check_arg(desc != nullptr && out != nullptr, "null argument");
+    *out = nullptr;
+    validate_desc(*desc);
+    DeviceGuard dg(desc->device_id);
+    auto prog = std::make_unique<gf_dedisp_program>();
+    gf_dedisp_program& P = *prog;
+    P.desc = *desc;
+    P.freq.assign(desc->frequency_mhz, desc->frequency_mhz + desc->nchans);
+    P.desc.frequency_mhz = P.freq.data();
+    const auto& d = P.desc;
+    P.nc = d.chan_end - d.chan_begin;
+    // internal/dedispersion_delay.h:129-139 multi_dm_max_delay
+    const double max_dm = d.dm_low + static_cast<double>(d.ndm - 1) * d.dm_step;
+    double fmin = P.freq[d.chan_begin];
+    for (uint64_t c = d.chan_begin; c < d.chan_end; ++c) fmin = std::min(fmin, P.freq[c]);
+    P.max_delay = delay_bins(max_dm, fmin, d.ref_frequency_mhz, d.tsamp);
+    check_arg(P.max_delay >= 0, "dedispersion requires non-negative delays");
+    check_arg(static_cast<uint64_t>(P.max_delay) < d.nsamples, "dedispersion valid output range is empty");
+    P.nout = d.nsamples - static_cast<uint64_t>(P.max_delay);
+    P.row_stride = round_up(d.nsamples, 16);
+    const int nc = static_cast<int>(P.nc);
+    if (d.algorithm == GF_DEDISP_BRUTE) {
+      std::vector<int32_t> delays(d.ndm * P.nc);
+      for (uint64_t dm = 0; dm < d.ndm; ++dm) {
+        const double v = d.dm_low + static_cast<double>(dm) * d.dm_step;
+        for (uint64_t c = 0; c < P.nc; ++c)
+          delays[dm * P.nc + c] = delay_bins(v, P.freq[d.chan_begin + c], d.ref_frequency_mhz, d.tsamp);
+      }
+      P.brute.build(delays, 1, static_cast<int>(d.ndm), nc, nc, d.device_id);
+    } else {
+      // dedispersion.cpp:360-388 subband geometry and tables
+      P.sbc = d.subband_channels;
+      P.npn = d.ndm_per_nominal;
+      P.nsb = ceil_div(P.nc, P.sbc);
+      P.nnom = ceil_div(d.ndm, P.npn);
+      std::vector<double> sbf(P.nsb);
+      for (uint64_t b = 0; b < P.nsb; ++b) {
+        const uint64_t begin = d.chan_begin + b * P.sbc;
+        const uint64_t end = std::min(begin + P.sbc, d.chan_end);
+        sbf[b] = P.freq[(begin + end - 1) / 2];
+      }
+      // stage 1: groups = subbands, "DMs" = nominal DMs, rows = subband channels
+      const int sbc = static_cast<int>(std::min<uint64_t>(P.sbc, P.nc));
+      std::vector<int32_t> coarse(P.nsb * P.nnom * sbc, 0);
+      for (uint64_t b = 0; b < P.nsb; ++b)
+        for (uint64_t n = 0; n < P.nnom; ++n) {
+          const double nominal = d.dm_low + static_cast<double>(n * P.npn) * d.dm_step;
+          for (int i = 0; i < sbc; ++i) {
+            const uint64_t c = b * P.sbc + i;
+            if (c >= P.nc) break;
+            coarse[(b * P.nnom + n) * sbc + i] =
+                delay_bins(nominal, P.freq[d.chan_begin + c], d.ref_frequency_mhz, d.tsamp);
+          }
+        }
+      P.stage1.build(coarse, static_cast<int>(P.nsb), static_cast<int>(P.nnom), sbc, nc, d.device_id);
+      // stage 2: groups = nominal DMs, "DMs" = final DMs, rows = subbands
+      P.resid.assign(P.nnom * P.npn * P.nsb, 0);
+      for (uint64_t dm = 0; dm < d.ndm; ++dm) {
+        const uint64_t n = dm / P.npn;
+        const double nominal = d.dm_low + static_cast<double>(n * P.npn) * d.dm_step;
+        const double fin = d.dm_low + static_cast<double>(dm) * d.dm_step;
+        for (uint64_t b = 0; b < P.nsb; ++b)
+          P.resid[dm * P.nsb + b] = delay_bins(fin - nominal, sbf[b], d.ref_frequency_mhz, d.tsamp);
+      }
+      // the last nominal group may be partial: pad with its last DM
+      for (uint64_t dm = d.ndm; dm < P.nnom * P.npn; ++dm)
+        for (uint64_t b = 0; b < P.nsb; ++b) P.resid[dm * P.nsb + b] = P.resid[(d.ndm - 1) * P.nsb + b];
+      for (int32_t r : P.resid) check_arg(r >= 0, "dedispersion requires non-negative delays");
+      P.inter_len = d.nsamples;
+      P.inter_u8 = (d.nbits == 2 ? 3ull : 255ull) * P.sbc <= 255ull;
+      if (P.inter_u8) {
+        P.inter_row_stride = round_up(P.inter_len, 16);
+        P.stage2.build(P.resid, static_cast<int>(P.nnom), static_cast<int>(P.npn),
+                       static_cast<int>(P.nsb), static_cast<int>(P.nnom * P.nsb), d.device_id);
+      } else {
+        P.inter_row_stride = round_up(P.inter_len, 4);
+        P.resid_dev.upload(P.resid.data(), P.resid.size() * sizeof(int32_t), d.device_id);
+      }
+    }
+    *out = prog.release();
+  });
+}
+
+extern "C" int gf_dedisp_program_destroy(gf_dedisp_program* program) {
+  return guarded([&] { delete program; });
+}
+
+extern "C" int gf_dedisp_program_info(const gf_dedisp_program* P, gf_dedisp_info* info) {
+  return guarded([&] {
+    check_arg(P != nullptr && info != nullptr, "null argument");
+    std::memset(info, 0, sizeof *info);
+    info->nout = P->nout;
+    info->max_delay = P->max_delay;
+    const uint64_t row_bytes = P->desc.nbits == 8 ? P->desc.nchans : P->desc.nchans / 4;
+    info->input_bytes = row_bytes * P->desc.nsamples;
+    info->staged_row_stride = P->row_stride;
+    info->staged_bytes = P->row_stride * P->nc;
+    if (P->desc.algorithm == GF_DEDISP_SUBBAND) {
+      const uint64_t elem = P->inter_u8 ? 1 : 4;
+      info->workspace_bytes = P->nnom * P->nsb * P->inter_row_stride * elem;
+    }
+    info->metadata_bytes = P->brute.base_dev.bytes + P->brute.rec_dev.bytes + P->stage1.base_dev.bytes +
+                           P->stage1.rec_dev.bytes + P->stage2.base_dev.bytes + P->stage2.rec_dev.bytes +
+                           P->resid_dev.bytes;
+  });
+}
+
+namespace {
+
+void launch_stage(const gf_dedisp_program& P, const uint8_t* in, uint64_t nsamples, uint8_t* out,
+                  uint64_t t_offset, cudaStream_t stream) {
+  const auto& d = P.desc;
+  const uint64_t row_bytes = d.nbits == 8 ? d.nchans : d.nchans / 4;
+  dim3 grid(static_cast<unsigned>(ceil_div(nsamples, 64)), static_cast<unsigned>(ceil_div(P.nc, 64)));
+  if (d.nbits == 8)
+    stage_kernel<8><<<grid, 256, 0, stream>>>(in, nsamples, row_bytes, static_cast<int>(d.chan_begin),
+                                              static_cast<int>(P.nc), out, P.row_stride, t_offset);
+  else
+    stage_kernel<2><<<grid, 256, 0, stream>>>(in, nsamples, row_bytes, static_cast<int>(d.chan_begin),
+                                              static_cast<int>(P.nc), out, P.row_stride, t_offset);
+  cuda_check(cudaGetLastError(), "stage_kernel launch");
+}
+
+}  // namespace
+
+extern "C" int gf_dedisp_stage(gf_dedisp_program* P, const void* dev_input, void* dev_staged, void* stream) {
+  return guarded([&] {
+    check_arg(P && dev_input && dev_staged, "null argument");
+    DeviceGuard dg(P->desc.device_id);
+    launch_stage(*P, static_cast<const uint8_t*>(dev_input), P->desc.nsamples,
+                 static_cast<uint8_t*>(dev_staged), 0, as_stream(stream));
+  });
+}
+
+extern "C" int gf_dedisp_stage_from_host(gf_dedisp_program* P, const void* host_input, void* dev_staged,
+                                         void* dev_bounce, uint64_t bounce_bytes, void* stream) {
+  return guarded([&] {
+    check_arg(P && host_input && dev_staged && dev_bounce, "null argument");
+    DeviceGuard dg(P->desc.device_id);
+    const uint64_t row_bytes = P->desc.nbits == 8 ? P->desc.nchans : P->desc.nchans / 4;
+    const uint64_t rows_per = (bounce_bytes / 2) / row_bytes;
+    check_arg(rows_per >= 64, "bounce buffer too small (needs 128 time rows)");
+    const uint64_t chunk = (rows_per / 64) * 64;
+    auto s = as_stream(stream);
+    uint8_t* bounce[2] = {static_cast<uint8_t*>(dev_bounce),
+                          static_cast<uint8_t*>(dev_bounce) + chunk * row_bytes};
+    const auto* host = static_cast<const uint8_t*>(host_input);
+    int k = 0;
+    for (uint64_t t = 0; t < P->desc.nsamples; t += chunk, k ^= 1) {
+      const uint64_t n = std::min(chunk, P->desc.nsamples - t);
+      cuda_check(cudaMemcpyAsync(bounce[k], host + t * row_bytes, n * row_bytes, cudaMemcpyHostToDevice, s),
+                 "cudaMemcpyAsync(stage)");
+      launch_stage(*P, bounce[k], n, static_cast<uint8_t*>(dev_staged), t, s);
+    }
+  });
+}
+
+extern "C" int gf_dedisp_run(gf_dedisp_program* P, const void* dev_staged, uint64_t dm_begin,
+                             uint64_t dm_count, uint32_t* dev_out, uint64_t out_stride,
+                             void* dev_workspace, void* stream) {
+  return guarded([&] {
+    check_arg(P && dev_staged && dev_out, "null argument");
+    const auto& d = P->desc;
+    check_arg(dm_count > 0 && dm_begin < d.ndm && dm_begin + dm_count <= d.ndm, "DM range out of bounds");
+    check_arg(out_stride >= P->nout, "out_stride must be >= nout");
+    DeviceGuard dg(d.device_id);
+    auto s = as_stream(stream);
+    const auto* staged = static_cast<const uint8_t*>(dev_staged);
+    if (d.algorithm == GF_DEDISP_BRUTE) {
+      check_arg(dm_begin % 8 == 0, "dm_begin must be a multiple of 8");
+      P->brute.run<uint32_t>(staged, P->row_stride, 0, d.nsamples, 0, 1, static_cast<int>(dm_begin),
+                             static_cast<int>(dm_count), static_cast<int>(dm_count), dev_out, out_stride,
+                             1, 0, P->nout, s);
+      return;
+    }
+    check_arg(dev_workspace != nullptr, "subband dedispersion needs a workspace");
+    check_arg(dm_begin % P->npn == 0, "subband dm_begin must be a multiple of ndm_per_nominal");
+    check_arg(dm_count % P->npn == 0 || dm_begin + dm_count == d.ndm,
+              "subband dm_count must be a multiple of ndm_per_nominal");
+    const uint64_t n0 = dm_begin / P->npn;
+    const uint64_t n1 = ceil_div(dm_begin + dm_count, P->npn);
+    // stage 1: nominal DMs [nb, ne) (block aligned) for every subband;
+    // workspace row (n - nb) * nsb + b
+    const auto& s1 = P->stage1;
+    const uint64_t dpc1 = s1.launch.dms_per_cta;
+    const uint64_t nb = (n0 / dpc1) * dpc1;
+    const uint64_t ne = std::min<uint64_t>(ceil_div(n1, dpc1) * dpc1, P->nnom);
+    uint8_t* inter = static_cast<uint8_t*>(dev_workspace);
+    const uint64_t elem = P->inter_u8 ? 1 : 4;
+    if (P->inter_u8)
+      s1.run<uint8_t>(staged, P->row_stride, P->sbc * P->row_stride, d.nsamples, 0,
+                      static_cast<int>(P->nsb), static_cast<int>(nb), static_cast<int>(ne - nb),
+                      static_cast<int>(ne - nb), inter, P->inter_row_stride, P->nsb, 1, P->inter_len, s);
+    else
+      s1.run<uint32_t>(staged, P->row_stride, P->sbc * P->row_stride, d.nsamples, 0,
+                       static_cast<int>(P->nsb), static_cast<int>(nb), static_cast<int>(ne - nb),
+                       static_cast<int>(ne - nb), inter, P->inter_row_stride, P->nsb, 1, P->inter_len, s);
+    const uint8_t* inter_n0 = inter + (n0 - nb) * P->nsb * P->inter_row_stride * elem;
+    const int last_cnt = static_cast<int>(std::min<uint64_t>(P->npn, d.ndm - (n1 - 1) * P->npn));
+    if (P->inter_u8) {
+      // stage 2: groups = nominal DMs [n0, n1), rows = subbands
+      P->stage2.run<uint32_t>(inter_n0, P->inter_row_stride, P->nsb * P->inter_row_stride, P->inter_len,
+                              static_cast<int>(n0), static_cast<int>(n1 - n0), 0, static_cast<int>(P->npn),
+                              last_cnt, dev_out, out_stride, 1, P->npn, P->nout, s);
+    } else {
+      const auto* inter32 = reinterpret_cast<const uint32_t*>(inter_n0);
+      for (uint64_t n = n0; n < n1; ++n) {
+        const uint64_t first = n * P->npn;
+        const uint64_t cnt = std::min(P->npn, d.ndm - first);
+        dim3 g2(static_cast<unsigned>(ceil_div(P->nout, 256)), static_cast<unsigned>(cnt), 1);
+        subband_stage2_u32_kernel<<<g2, 256, 0, s>>>(
+            inter32 + (n - n0) * P->nsb * P->inter_row_stride, P->inter_row_stride, 0, P->inter_len,
+            static_cast<int>(P->nsb), P->resid_dev.as<int32_t>() + first * P->nsb, static_cast<int>(cnt),
+            dev_out + (first - dm_begin) * out_stride, out_stride, P->nout);
+      }
+      cuda_check(cudaGetLastError(), "subband stage 2 launch");
+    }
+  });
+}
+
+extern "C" int gf_dedisp_workspace_bytes(const gf_dedisp_program* P, uint64_t dm_count, uint64_t* bytes) {
+  return guarded([&] {
+    check_arg(P && bytes, "null argument");
+    *bytes = 0;
+    if (P->desc.algorithm != GF_DEDISP_SUBBAND) return;
+    const uint64_t dpc1 = P->stage1.launch.dms_per_cta;
+    const uint64_t groups = std::min<uint64_t>(ceil_div(dm_count, P->npn) + 2 * dpc1, P->nnom + dpc1);
+    *bytes = groups * P->nsb * P->inter_row_stride * (P->inter_u8 ? 1 : 4);
+  });
+}

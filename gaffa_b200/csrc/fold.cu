@@ -1,0 +1,138 @@
+// Folding of a dedispersed time series into phase bins on sm_100a.
+//
+// Reference: fold_time_series_cpu, src/gaffa/folding.cpp:452-502 with
+// accumulate_interval :124-158.  Sample i covers the scaled phase interval
+// [(start+i)*step, (start+i+1)*step), step = tsamp / period * nbin; each bin
+// it overlaps receives value * overlap and overlap of exposure (FP64);
+// profile = sums / exposure.  The reference has no CUDA path for this.
+//
+// Each thread folds a contiguous run of samples, carrying the current bin's
+// partial sums in registers and flushing them to shared-memory FP64
+// accumulators when the bin changes; CTA partials are reduced in a fixed
+// order by a second kernel.  Like the reference's per-thread OpenMP
+// histograms, the FP64 summation order differs from a serial loop, so
+// results agree to FP64 rounding (the float profile to within an ulp).
+#include "common.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace gf {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSamplesPerThread = 64;
+constexpr uint64_t kMaxBins = 8192;
+
+template <bool U32>
+__global__ void __launch_bounds__(kThreads) fold_partial_kernel(const void* __restrict__ in, uint64_t n,
+                                                                double step, uint64_t start, uint64_t nbin,
+                                                                double* __restrict__ partial,
+                                                                uint32_t* status) {
+  extern __shared__ double acc[];  // [2][nbin]
+  double* sums = acc;
+  double* expo = acc + nbin;
+  for (uint64_t b = threadIdx.x; b < 2 * nbin; b += kThreads) acc[b] = 0.0;
+  __syncthreads();
+  const uint64_t i0 = (static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x) * kSamplesPerThread;
+  const int64_t nb = static_cast<int64_t>(nbin);
+  int64_t cur = -1;
+  double cs = 0.0, ce = 0.0;
+  for (uint64_t i = i0; i < n && i < i0 + kSamplesPerThread; ++i) {
+    const double v = U32 ? static_cast<double>(static_cast<const uint32_t*>(in)[i])
+                         : static_cast<double>(static_cast<const float*>(in)[i]);
+    if (!U32 && !isfinite(v)) atomicOr(status, GF_STATUS_NONFINITE);
+    const double lo = __dmul_rn(static_cast<double>(start + i), step);
+    const double hi = __dadd_rn(lo, step);
+    const int64_t first = static_cast<int64_t>(floor(lo));
+    const int64_t last = static_cast<int64_t>(ceil(hi) - 1.0);
+    for (int64_t bin = first; bin <= last; ++bin) {
+      const double bl = static_cast<double>(bin), br = bl + 1.0;
+      const double w = __dsub_rn(hi < br ? hi : br, lo > bl ? lo : bl);
+      if (!(w > 0.0)) continue;
+      int64_t m = bin % nb;
+      if (m < 0) m += nb;
+      if (m != cur) {
+        if (cur >= 0) {
+          atomicAdd(sums + cur, cs);
+          atomicAdd(expo + cur, ce);
+        }
+        cur = m;
+        cs = 0.0;
+        ce = 0.0;
+      }
+      cs = __dadd_rn(cs, __dmul_rn(v, w));
+      ce = __dadd_rn(ce, w);
+    }
+  }
+  if (cur >= 0) {
+    atomicAdd(sums + cur, cs);
+    atomicAdd(expo + cur, ce);
+  }
+  __syncthreads();
+  double* out = partial + static_cast<uint64_t>(blockIdx.x) * 2 * nbin;
+  for (uint64_t b = threadIdx.x; b < 2 * nbin; b += kThreads) out[b] = acc[b];
+}
+
+__global__ void __launch_bounds__(kThreads) fold_reduce_kernel(const double* __restrict__ partial, int nblocks,
+                                                               uint64_t nbin, float* __restrict__ profile,
+                                                               double* __restrict__ exposure) {
+  const uint64_t b = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+  if (b >= nbin) return;
+  double s = 0.0, e = 0.0;
+  for (int k = 0; k < nblocks; ++k) {
+    s = __dadd_rn(s, partial[static_cast<uint64_t>(k) * 2 * nbin + b]);
+    e = __dadd_rn(e, partial[static_cast<uint64_t>(k) * 2 * nbin + nbin + b]);
+  }
+  exposure[b] = e;
+  profile[b] = e > 0.0 ? static_cast<float>(__ddiv_rn(s, e)) : 0.0f;
+}
+
+uint64_t fold_blocks(uint64_t n) { return ceil_div(n, static_cast<uint64_t>(kThreads) * kSamplesPerThread); }
+
+}  // namespace
+}  // namespace gf
+
+using namespace gf;
+
+extern "C" uint64_t gf_fold_workspace_bytes(uint64_t n, uint64_t nbin) {
+  return fold_blocks(n) * 2 * nbin * sizeof(double) + 16;
+}
+
+extern "C" int gf_fold_time_series(const void* dev_input, int32_t input_is_u32, uint64_t n, double period,
+                                   double tsamp, uint64_t nbin, uint64_t start_sample, float* dev_profile,
+                                   double* dev_exposure, void* dev_workspace, void* stream) {
+  return guarded([&] {
+    // folding.cpp:44-73 validation
+    check_arg(std::isfinite(period) && period > 0.0, "fold period must be finite and positive");
+    check_arg(std::isfinite(tsamp) && tsamp > 0.0, "fold tsamp must be finite and positive");
+    check_arg(nbin > 0, "fold nbin must be positive");
+    check_arg(nbin <= kMaxBins, "CUDA fold supports nbin <= 8192");
+    check_arg(n > 0, "fold input must not be empty");
+    check_arg(dev_input && dev_profile && dev_exposure && dev_workspace, "null argument");
+    const double step = tsamp / period * static_cast<double>(nbin);
+    const double hi = static_cast<double>(start_sample + n - 1) * step + step;
+    check_arg(std::isfinite(hi) && std::ceil(hi) < 9.2e18, "fold phase bin index exceeds int64 range");
+    auto s = as_stream(stream);
+    const uint64_t blocks = fold_blocks(n);
+    check_arg(blocks < (1ull << 31), "fold input too long");
+    double* partial = static_cast<double*>(dev_workspace);
+    uint32_t* status = reinterpret_cast<uint32_t*>(static_cast<char*>(dev_workspace) + blocks * 2 * nbin * 8);
+    cuda_check(cudaMemsetAsync(status, 0, 4, s), "cudaMemsetAsync(fold status)");
+    const size_t smem = 2 * nbin * sizeof(double);
+    if (input_is_u32) {
+      cuda_check(cudaFuncSetAttribute(fold_partial_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(smem)), "cudaFuncSetAttribute(fold)");
+      fold_partial_kernel<true><<<static_cast<unsigned>(blocks), kThreads, smem, s>>>(
+          dev_input, n, step, start_sample, nbin, partial, status);
+    } else {
+      cuda_check(cudaFuncSetAttribute(fold_partial_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(smem)), "cudaFuncSetAttribute(fold)");
+      fold_partial_kernel<false><<<static_cast<unsigned>(blocks), kThreads, smem, s>>>(
+          dev_input, n, step, start_sample, nbin, partial, status);
+    }
+    fold_reduce_kernel<<<static_cast<unsigned>(ceil_div(nbin, kThreads)), kThreads, 0, s>>>(
+        partial, static_cast<int>(blocks), nbin, dev_profile, dev_exposure);
+    cuda_check(cudaGetLastError(), "fold launch");
+  });
+}

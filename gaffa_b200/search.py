@@ -1,0 +1,158 @@
+"""The DM-search pipeline on one GPU: filterbank -> dedispersion -> detrend +
+normalise -> per-octave downsampling + FFA + boxcar S/N -> peaks ->
+candidates -> fold of the best candidate.
+
+This is the chain the reference wires up in
+benchmarks/cuda_dm_search_benchmark.cpp:179-260 (plus select_candidates_cpu
+and fold_time_series_cpu), built on the device programs of core.py.  The
+filterbank is staged once; DM trials are processed in batches so the
+dedispersed block, the prepared octaves and the FFA scratch stay within a
+fixed memory budget.
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+
+import numpy as np
+import torch
+
+from . import _lib, core
+
+
+@dataclasses.dataclass
+class SearchResult:
+    peaks: np.ndarray            # PEAK_DTYPE, sorted by is_better_dm_peak
+    candidates: np.ndarray       # CAND_DTYPE
+    fold_profile: np.ndarray | None
+    fold_exposure: np.ndarray | None
+    nout: int
+    ndm: int
+    timings: dict
+    gpu_launches: int = 0
+
+    @property
+    def dm_trial_samples(self) -> int:
+        return self.ndm * self.nout
+
+
+class DmSearch:
+    """A reusable search for one observation geometry and set of options."""
+
+    def __init__(self, frequency_mhz, nsamples: int, tsamp: float, dm_low: float, dm_step: float, ndm: int,
+                 period_min: float, period_max: float, bins_min: int = 180, bins_max: int = 256,
+                 duty_cycle_max: float = 0.2, width_trials=None, window_seconds: float = 1.0,
+                 min_points: int = 101, snr_threshold: float = 8.0, nbits: int = 8,
+                 algorithm: str = "brute", subband_channels: int = 32, ndm_per_nominal: int = 32,
+                 frequency_cluster_radius: float = 0.1, dm_cluster_radius: int = 1, fold_nbin: int = 64,
+                 dm_batch: int | None = None, memory_budget: int | None = None, device_id: int = 0):
+        self.device = torch.device("cuda", device_id)
+        self.nsamples, self.tsamp = nsamples, tsamp
+        self.dm_low, self.dm_step, self.ndm = dm_low, dm_step, ndm
+        self.snr_threshold = snr_threshold
+        self.frequency_cluster_radius = frequency_cluster_radius
+        self.dm_cluster_radius = dm_cluster_radius
+        self.fold_nbin = fold_nbin
+        self.dedisp = core.DedispersionProgram(frequency_mhz, nsamples, tsamp, dm_low, dm_step, ndm, nbits=nbits,
+                                               algorithm=algorithm, subband_channels=subband_channels,
+                                               ndm_per_nominal=ndm_per_nominal, device_id=device_id)
+        self.nout = self.dedisp.nout
+        plan = core.make_riptide_ffa_plan(self.nout, tsamp, period_min, period_max, bins_min=bins_min,
+                                          bins_max=bins_max, duty_cycle_max=duty_cycle_max)
+        if width_trials is not None:
+            plan = plan.with_widths(width_trials)
+        self.plan = plan
+        self.out_stride = ((self.nout + 3) // 4) * 4
+        g = self.dedisp.batch_granularity
+        if dm_batch is None:
+            free = torch.cuda.mem_get_info(self.device)[0] if memory_budget is None else memory_budget
+            per_dm = self.out_stride * 4 + self._prepared_floats_estimate() * 4
+            budget = int(free * 0.45) - self.dedisp.info.staged_bytes - (1 << 30)
+            dm_batch = max(g, min(ndm, budget // max(1, per_dm)))
+        dm_batch = max(g, (dm_batch // g) * g)
+        self.dm_batch = min(dm_batch, ((ndm + g - 1) // g) * g)
+        self.pre = core.PreprocessProgram(self.nout, tsamp, window_seconds=window_seconds, min_points=min_points,
+                                          normalise=True, reject_constant=True, max_series=self.dm_batch,
+                                          device_id=device_id)
+        self.ffa = core.FfaProgram(plan, max_series=self.dm_batch, device_id=device_id)
+        self._series = torch.empty(self.dm_batch * self.out_stride, dtype=torch.int32, device=self.device)
+        self._prepared = torch.empty((self.dm_batch, self.ffa.prepared_floats), dtype=torch.float32,
+                                     device=self.device)
+        self._workspace = None
+        if algorithm == "subband":
+            self._workspace = torch.empty(self.dedisp.workspace_bytes(self.dm_batch), dtype=torch.uint8,
+                                          device=self.device)
+
+    def _prepared_floats_estimate(self) -> int:
+        # upper bound used before the FFA program exists: sum over octaves of
+        # nout / factor is below nout for factors > 1
+        return self.nout + 64
+
+    def stage(self, filterbank) -> torch.Tensor:
+        return self.dedisp.stage(filterbank)
+
+    def search_staged(self, staged: torch.Tensor, timings: dict | None = None) -> tuple:
+        """Runs every DM batch; returns (raw peaks, launches)."""
+        timings = {} if timings is None else timings
+        parts = []
+        launches = 0
+        for b0 in range(0, self.ndm, self.dm_batch):
+            cnt = min(self.dm_batch, self.ndm - b0)
+            dd = self.dedisp.run(staged, b0, cnt, out=self._series, out_stride=self.out_stride,
+                                 workspace=self._workspace)
+            stats = self.pre.run(dd, cnt)
+            self.ffa.prepare(dd.view(torch.float32), cnt, stats, out=self._prepared)
+            rec = self.ffa.search(self._prepared, cnt, self.snr_threshold)
+            parts.append(self.ffa.expand(rec, b0, self.dm_low, self.dm_step))
+            launches += 1 + 4 + 1 + 2
+        self.pre.synchronize()
+        peaks = np.concatenate(parts) if parts else np.zeros(0, _lib.PEAK_DTYPE)
+        return peaks, launches
+
+    def fold_candidate(self, staged: torch.Tensor, dm_index: int, period: float):
+        """fold_time_series of the candidate's uint32 dedispersed series."""
+        g = self.dedisp.batch_granularity
+        b0 = (dm_index // g) * g
+        cnt = min(g, self.ndm - b0)
+        ws = None
+        if self.dedisp.algorithm == "subband":
+            ws = torch.empty(self.dedisp.workspace_bytes(cnt), dtype=torch.uint8, device=self.device)
+        dd = self.dedisp.run(staged, b0, cnt, out_stride=self.out_stride, workspace=ws)
+        row = dd[dm_index - b0, : self.nout]
+        return core.fold_time_series(row, period, self.tsamp, self.fold_nbin)
+
+    def run(self, filterbank, observation_seconds: float | None = None) -> SearchResult:
+        t = {}
+        t0 = time.perf_counter()
+        staged = self.stage(filterbank)
+        torch.cuda.synchronize(self.device)
+        t1 = time.perf_counter()
+        peaks, launches = self.search_staged(staged, t)
+        t2 = time.perf_counter()
+        peaks = core.sort_peaks(peaks)
+        tobs = self.nsamples * self.tsamp if observation_seconds is None else observation_seconds
+        cands = core.select_candidates(peaks, tobs, self.frequency_cluster_radius, self.dm_cluster_radius)
+        t3 = time.perf_counter()
+        prof = expo = None
+        if len(cands):
+            prof, expo = self.fold_candidate(staged, int(cands[0]["dm_index"]), float(cands[0]["period"]))
+            launches += 3
+        t4 = time.perf_counter()
+        t.update(stage=t1 - t0, search=t2 - t1, candidates=t3 - t2, fold=t4 - t3, total=t4 - t0)
+        return SearchResult(peaks=peaks, candidates=cands, fold_profile=prof, fold_exposure=expo, nout=self.nout,
+                            ndm=self.ndm, timings=t, gpu_launches=launches + 1)
+
+
+def from_config(cfg, **overrides) -> DmSearch:
+    """A DmSearch for a configs.SearchConfig workload."""
+    obs = cfg.obs
+    kw = dict(frequency_mhz=obs.frequencies, nsamples=obs.nsamples, tsamp=obs.tsamp, dm_low=cfg.dm_low,
+              dm_step=cfg.dm_step, ndm=cfg.ndm, period_min=cfg.period_min, period_max=cfg.period_max,
+              bins_min=cfg.bins_min, bins_max=cfg.bins_max, duty_cycle_max=cfg.duty_cycle_max,
+              width_trials=cfg.width_trials, window_seconds=cfg.window_seconds, min_points=cfg.min_points,
+              snr_threshold=cfg.snr_threshold, nbits=obs.nbits, algorithm=cfg.dedispersion,
+              subband_channels=cfg.subband_channels, ndm_per_nominal=cfg.ndm_per_nominal,
+              frequency_cluster_radius=cfg.frequency_cluster_radius, dm_cluster_radius=cfg.dm_cluster_radius,
+              fold_nbin=cfg.fold_nbin)
+    kw.update(overrides)
+    return DmSearch(**kw)

@@ -113,7 +113,8 @@ def pulse_units(obs: Observation, t: np.ndarray, c: np.ndarray) -> np.ndarray:
         ph = (tt - delay) / p.period - p.phase
         ph = ph - np.floor(ph + 0.5)
         sigma = p.duty_cycle / 2.3548200450309493
-        total += p.amplitude * np.exp(-0.5 * (ph / sigma) ** 2)
+        x = ph / sigma
+        total += np.where(np.abs(x) < 12.0, p.amplitude * np.exp(-0.5 * (x * x)), 0.0)
     r = obs.rfi
     if r.narrowband_fraction > 0.0:
         nb = _narrowband_mask(obs)[c]

@@ -1,0 +1,397 @@
+/*
+ * gaffa_b200.h -- C ABI of the B200 (sm_100a) pulsar-search hot path.
+ *
+ * The library libgaffa_b200.so implements gaffa's search path -- brute-force
+ * and subband dedispersion, running-median detrend + normalise, per-octave
+ * downsampling, the FFA transform, boxcar S/N detection, candidate selection
+ * and folding -- as hand-written CUDA kernels for sm_100a behind this plain C
+ * interface: POD structs, int status codes, caller-owned device buffers and an
+ * explicit cudaStream_t (passed as void*).  Nothing here throws, allocates
+ * result memory for the caller, or synchronises implicitly unless stated.
+ *
+ * Each entry point names the reference interface it replaces
+ * (lintian233/gaffa, path:line relative to that project).
+ *
+ * Status: 0 = success; negative values are error classes (GF_E*);
+ * gf_last_error() returns the thread's last message.
+ */
+#ifndef GAFFA_B200_H
+#define GAFFA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GF_OK 0
+#define GF_EINVAL -1    /* std::invalid_argument */
+#define GF_EOVERFLOW -2 /* std::overflow_error */
+#define GF_ERUNTIME -3  /* std::runtime_error (guards, max_tasks) */
+#define GF_ENOMEM -4    /* device or host allocation failed */
+#define GF_ECUDA -5     /* CUDA runtime error (message has the CUDA string) */
+#define GF_EDATA -6     /* deferred data error reported by a device status word */
+#define GF_EOVERFLOW_PEAKS -7 /* peak buffer too small; count says how many */
+
+/* Device status word bits (written by kernels with atomicOr). */
+#define GF_STATUS_NONFINITE 1u
+#define GF_STATUS_CONSTANT 2u
+#define GF_STATUS_PEAK_OVERFLOW 4u
+
+const char* gf_last_error(void);
+const char* gf_status_string(int status);
+/* Library build description (architecture, kernel list) for diagnostics. */
+const char* gf_build_info(void);
+
+/* ------------------------------------------------------------------------ */
+/* FFA plan (host)                                                           */
+/* ------------------------------------------------------------------------ */
+
+/* Same fields and meaning as FfaSearchTask, include/gaffa/ffa_plan.h:8-32. */
+typedef struct {
+  double downsample_factor;
+  double effective_tsamp;
+  uint64_t input_nsamples;
+  uint64_t prepared_nsamples;
+  uint64_t bins;
+  uint64_t rows;
+  uint64_t rows_eval;
+  double period_begin;
+  double period_end;
+} gf_ffa_task;
+
+/* RiptideFfaPlanOptions, include/gaffa/ffa_plan.h:34-47. */
+typedef struct {
+  double period_min;
+  double period_max;
+  uint64_t bins_min;
+  uint64_t bins_max;
+  uint64_t min_periods;
+  double duty_cycle_max;
+  double width_trial_spacing;
+  uint64_t max_tasks;
+} gf_plan_options;
+
+/* Replaces make_riptide_ffa_plan, src/gaffa/ffa_plan.cpp:90-170.
+ * Two-call pattern: pass capacities of 0 to learn ntasks / nwidths. */
+int gf_make_riptide_ffa_plan(uint64_t nsamples, double tsamp,
+                             const gf_plan_options* options, gf_ffa_task* tasks,
+                             uint64_t task_capacity, uint64_t* ntasks,
+                             uint64_t* widths, uint64_t width_capacity,
+                             uint64_t* nwidths);
+
+/* Replaces downsampled_size / downsampled_variance,
+ * src/gaffa/time_series.cpp:118-138, and ffa_task_stdnoise,
+ * src/gaffa/ffa_detection.cpp:256-264. */
+int gf_downsampled_size(uint64_t nsamples, double factor, uint64_t* out);
+int gf_downsampled_variance(uint64_t nsamples, double factor, double* out);
+int gf_ffa_task_stdnoise(const gf_ffa_task* task, float* out);
+
+/* ------------------------------------------------------------------------ */
+/* Dedispersion                                                              */
+/* ------------------------------------------------------------------------ */
+
+#define GF_DEDISP_BRUTE 0
+#define GF_DEDISP_SUBBAND 1
+
+/* MultiDmDedispersionPlan (include/gaffa/dedispersion.h:24-32) plus
+ * SubbandDedispersionOptions (:34-37), the sample type and the device. */
+typedef struct {
+  uint64_t nsamples;
+  uint64_t nchans;
+  const double* frequency_mhz; /* host pointer, nchans entries */
+  double dm_low;
+  double dm_step;
+  uint64_t ndm;
+  double ref_frequency_mhz;
+  double tsamp;
+  uint64_t chan_begin;
+  uint64_t chan_end;
+  int32_t nbits;      /* 8: uint8 [time][chan]; 2: packed, 4 channels per byte,
+                         channel 4k+j in bits [2j, 2j+1] of byte k */
+  int32_t algorithm;  /* GF_DEDISP_BRUTE or GF_DEDISP_SUBBAND */
+  uint64_t subband_channels; /* subband only */
+  uint64_t ndm_per_nominal;  /* subband only */
+  int32_t device_id;
+  int32_t reserved;
+} gf_dedisp_desc;
+
+typedef struct {
+  uint64_t nout;               /* valid output samples per DM */
+  int32_t max_delay;           /* delay of the highest DM at the lowest channel */
+  int32_t reserved;
+  uint64_t input_bytes;        /* bytes of the time-major input */
+  uint64_t staged_bytes;       /* bytes of the channel-major staging buffer */
+  uint64_t staged_row_stride;  /* bytes between channel rows of the staging buffer */
+  uint64_t workspace_bytes;    /* scratch for gf_dedisp_run (subband intermediate) */
+  uint64_t metadata_bytes;     /* device tables owned by the program */
+} gf_dedisp_info;
+
+typedef struct gf_dedisp_program gf_dedisp_program;
+
+/* Builds the delay tables of internal/dedispersion_delay.h:37-139 (FP64,
+ * round half away from zero) and dedispersion.cpp:141-189 on the host, sorts
+ * them into the per-warp gather records the kernels use and uploads them.
+ * Replaces the delay kernels of src/gaffa/dedispersion_cuda.cu:190-267. */
+int gf_dedisp_program_create(const gf_dedisp_desc* desc, gf_dedisp_program** out);
+int gf_dedisp_program_destroy(gf_dedisp_program* program);
+int gf_dedisp_program_info(const gf_dedisp_program* program, gf_dedisp_info* info);
+
+/* Stage a device-resident time-major input ([nsamples][nchans] uint8, or the
+ * packed 2-bit rows) into the channel-major uint8 layout the kernels read
+ * (staged_bytes).  Counterpart of the H2D + layout step inside
+ * dedisperse_*_cuda_device, dedispersion_cuda.cu:587-714. */
+int gf_dedisp_stage(gf_dedisp_program* program, const void* dev_input,
+                    void* dev_staged, void* stream);
+/* Stage a host time-major input in chunks through pinned host memory. */
+int gf_dedisp_stage_from_host(gf_dedisp_program* program, const void* host_input,
+                              void* dev_staged, void* dev_bounce,
+                              uint64_t bounce_bytes, void* stream);
+
+/* Dedisperse DMs [dm_begin, dm_begin + dm_count) into dev_out
+ * ([dm_count][out_stride] uint32, out_stride >= nout).  Bit-exact with
+ * dedisperse_multi_dm_cpu (dedispersion.cpp:291-329) or
+ * dedisperse_subband_cpu (:331-453).  Replaces multi_dm_kernel and
+ * subband_stage1/2_kernel, dedispersion_cuda.cu:320-417.  Subband runs need
+ * dm_begin / dm_count aligned to ndm_per_nominal (except at the end). */
+int gf_dedisp_run(gf_dedisp_program* program, const void* dev_staged,
+                  uint64_t dm_begin, uint64_t dm_count, uint32_t* dev_out,
+                  uint64_t out_stride, void* dev_workspace, void* stream);
+/* Workspace bytes gf_dedisp_run needs for a batch of dm_count DMs (0 for
+ * brute force; the subband intermediate otherwise).  Brute-force batches start
+ * at multiples of 8 DMs, subband batches at multiples of ndm_per_nominal. */
+int gf_dedisp_workspace_bytes(const gf_dedisp_program* program, uint64_t dm_count,
+                              uint64_t* bytes);
+
+/* ------------------------------------------------------------------------ */
+/* Preprocessing: running-median detrend + normalise                         */
+/* ------------------------------------------------------------------------ */
+
+/* RiptidePreprocessOptions (include/gaffa/preprocessing.h:37-42) evaluated
+ * for one tsamp, as make_riptide_preprocess_plan (preprocessing.cpp:190-210). */
+typedef struct {
+  double tsamp;
+  double window_seconds;
+  uint64_t min_points;
+  int32_t normalise;
+  int32_t reject_constant;
+  uint64_t nsamples;   /* series length */
+  uint64_t max_series; /* workspace is sized for this many series */
+} gf_preprocess_desc;
+
+typedef struct {
+  uint64_t window_samples;
+  uint64_t scrunch_factor;  /* 1 = exact running median */
+  uint64_t low_nsamples;    /* scrunched length */
+  uint64_t workspace_bytes;
+} gf_preprocess_info;
+
+int gf_preprocess_info_get(const gf_preprocess_desc* desc, gf_preprocess_info* info);
+
+/* In place on [nseries][stride] 32-bit series (input_is_u32 = 1: uint32 sums
+ * from gf_dedisp_run, converted exactly to float as dm_search.cpp:53-68; 0:
+ * float).  On return the buffer holds float detrended values
+ * (preprocessing.cpp:212-231) and dev_stats[2*s] / [2*s+1] hold the FP64 mean
+ * and 1/stddev of time_series_stats_cpu (time_series.cpp:50-78); the
+ * normalisation itself is applied by gf_normalise or fused into
+ * gf_ffa_prepare.  Data errors set bits in *dev_status (deferred, as
+ * preprocessing_cuda.cu:269-272,781-817).  Replaces
+ * preprocess_time_series_batch_inplace_cuda, preprocessing_cuda.cu:819-864. */
+int gf_preprocess_inplace(const gf_preprocess_desc* desc, void* dev_series,
+                          int32_t input_is_u32, uint64_t nseries, uint64_t stride,
+                          void* dev_workspace, double* dev_stats,
+                          uint32_t* dev_status, void* stream);
+/* x <- float((x - mean) * (1/stddev)) (time_series.cpp:98-103); zeroes
+ * constant series when reject_constant == 0. */
+int gf_normalise(float* dev_series, uint64_t nseries, uint64_t stride,
+                 uint64_t nsamples, const double* dev_stats, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* FFA search                                                                */
+/* ------------------------------------------------------------------------ */
+
+typedef struct gf_ffa_program gf_ffa_program;
+
+typedef struct {
+  uint64_t ntasks;
+  uint64_t noctaves;            /* distinct downsample factors (prepare groups) */
+  uint64_t prepared_floats;     /* per series, all octaves */
+  uint64_t scratch_bytes;       /* per gf_ffa_search call */
+  uint64_t max_task_elements;   /* rows * bins of the largest task */
+  uint64_t metadata_bytes;
+} gf_ffa_info;
+
+/* Compact device peak record (24 bytes); FfaCudaPeak of
+ * src/gaffa/ffa_cuda_kernels.cuh:70-99 in spirit. */
+typedef struct {
+  uint32_t series;
+  uint32_t task;
+  uint32_t shift;
+  uint16_t phase;
+  uint16_t width_index;
+  float snr;
+  uint32_t reserved;
+} gf_peak_record;
+
+/* Host peak: DmPeak{dm, dm_index, FfaPeak} (dm_search.h:16-20,
+ * ffa_peak.h:8-19); same layout as the oracle's gfo_peak. */
+typedef struct {
+  double dm;
+  uint64_t dm_index;
+  double period;
+  double frequency;
+  uint64_t width;
+  double duty_cycle;
+  uint64_t width_index;
+  uint64_t period_index;
+  uint64_t phase;
+  uint64_t shift;
+  uint64_t bins;
+  float snr;
+  uint32_t reserved;
+} gf_peak;
+
+/* Replaces CudaFfaProgram + make_ffa_cuda_execution_plan,
+ * src/gaffa/ffa_cuda_executor.cuh:44-80,144-210.  Uploads the task tables,
+ * the boxcar trials (ffa_detection.cpp:60-80) and the per-octave prepare
+ * tables; the program owns only metadata. */
+int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks,
+                          const uint64_t* widths, uint64_t nwidths,
+                          uint64_t max_series, int32_t device_id,
+                          gf_ffa_program** out);
+int gf_ffa_program_destroy(gf_ffa_program* program);
+int gf_ffa_program_info(const gf_ffa_program* program, gf_ffa_info* info);
+
+/* Per-octave weighted-sum downsampling of every series
+ * (downsample_weighted_sum_cpu, time_series.cpp:140-174, with the
+ * ffa_executor.cpp:99-115 cache) into dev_prepared
+ * ([nseries][prepared_floats]).  When dev_stats is given the normalisation
+ * float((x - mean) * scale) is applied on the fly to each input sample.
+ * Replaces prepare_ffa_input_cuda, ffa_cuda_executor.cuh:277-305, and
+ * downsample_weighted_sum_float_kernel, time_series_cuda.cu:15-48. */
+int gf_ffa_prepare(gf_ffa_program* program, const float* dev_series,
+                   uint64_t nseries, uint64_t stride, const double* dev_stats,
+                   float* dev_prepared, void* stream);
+
+/* FFA transform of every task of every series followed by boxcar S/N
+ * detection on the rows_eval final rows (ffa.cpp:127-251,
+ * ffa_detection.cpp:126-372); peaks with S/N >= snr_threshold are appended
+ * to dev_peaks.  dev_counters[0] receives the number of peaks found (which
+ * may exceed capacity: then GF_STATUS_PEAK_OVERFLOW is set in
+ * dev_counters[1] and the caller re-runs with a larger buffer).  Replaces
+ * run_ffa_batch_cuda, ffa_cuda_executor.cuh:368-678, and the transform /
+ * detection kernels of ffa_cuda_kernels.cuh:130-737.  dev_scratch must hold
+ * scratch_bytes. */
+int gf_ffa_search(gf_ffa_program* program, const float* dev_prepared,
+                  uint64_t nseries, float snr_threshold, void* dev_scratch,
+                  gf_peak_record* dev_peaks, uint64_t capacity,
+                  uint64_t* dev_counters, void* stream);
+
+/* Expands compact records into host peaks (make_ffa_peak,
+ * ffa_detection.cpp:266-284); dm = dm_low + (series + series_offset) *
+ * dm_step as cuda_dm_search_benchmark.cpp:255-258. */
+int gf_ffa_expand_peaks(const gf_ffa_program* program,
+                        const gf_peak_record* records, uint64_t n,
+                        uint64_t series_offset, double dm_low, double dm_step,
+                        gf_peak* out);
+
+/* One materialised FFA transform of [rows][bins] floats (ffa_transform_cpu /
+ * ffa_transform_block_cuda, ffa.cpp:342-417, ffa_cuda.h:254-264).
+ * dev_scratch needs rows * bins * 8 bytes. */
+int gf_ffa_transform(const float* dev_input, uint64_t rows, uint64_t bins,
+                     float* dev_output, void* dev_scratch, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Host post-processing                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* Sort by is_better_dm_peak (dm_search.cpp:89-100 over ffa_peak.cpp:16-45). */
+int gf_sort_peaks(gf_peak* peaks, uint64_t n);
+
+/* CandidateSelectionOptions, include/gaffa/candidate.h:30-39. */
+typedef struct {
+  double frequency_cluster_radius;
+  uint64_t dm_cluster_radius;
+  int32_t cluster_across_widths;
+  int32_t reserved;
+  uint64_t max_candidates;
+} gf_candidate_options;
+
+/* Candidate, include/gaffa/candidate.h:11-28 (same layout as gfo_candidate). */
+typedef struct {
+  double dm;
+  uint64_t dm_index;
+  double period;
+  double frequency;
+  uint64_t width;
+  double duty_cycle;
+  float snr;
+  uint32_t reserved;
+  uint64_t peak_count;
+  uint64_t dm_index_min;
+  uint64_t dm_index_max;
+  double frequency_min;
+  double frequency_max;
+  gf_peak best_peak;
+} gf_candidate;
+
+/* Replaces select_candidates_cpu, src/gaffa/candidate.cpp:175-212.
+ * Two-call pattern on capacity. */
+int gf_select_candidates(const gf_peak* peaks, uint64_t npeaks,
+                         double observation_seconds,
+                         const gf_candidate_options* options,
+                         gf_candidate* out, uint64_t capacity,
+                         uint64_t* ncandidates);
+
+/* ------------------------------------------------------------------------ */
+/* Folding                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces fold_time_series_cpu (src/gaffa/folding.cpp:452-502), which has no
+ * CUDA path in the reference: FP64 fractional phase-overlap accumulation into
+ * nbin bins; profile = sums / exposure.  Device input, device outputs
+ * (dev_profile: nbin floats, dev_exposure: nbin doubles).  dev_workspace
+ * needs gf_fold_workspace_bytes(n, nbin); the uint32 at byte offset
+ * gf_fold_workspace_bytes(n, nbin) - 16 receives GF_STATUS_NONFINITE when a
+ * float input sample is not finite (the reference rejects such input). */
+uint64_t gf_fold_workspace_bytes(uint64_t n, uint64_t nbin);
+int gf_fold_time_series(const void* dev_input, int32_t input_is_u32, uint64_t n,
+                        double period, double tsamp, uint64_t nbin,
+                        uint64_t start_sample, float* dev_profile,
+                        double* dev_exposure, void* dev_workspace, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic observations (no reference counterpart)                         */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  double period, dm, duty_cycle, amplitude, phase;
+} gf_synth_pulsar;
+
+typedef struct {
+  uint64_t nchans;
+  uint64_t nsamples;
+  double tsamp;
+  double f_low;
+  double f_high;
+  int32_t nbits;  /* 8 or 2 (2: packed output, nchans % 4 == 0) */
+  int32_t npulsars;
+  uint64_t seed;
+  const gf_synth_pulsar* pulsars; /* host pointer */
+  double narrowband_fraction, narrowband_hz, narrowband_amplitude;
+  double impulse_hz, impulse_amplitude;
+  const uint8_t* narrowband_mask; /* host pointer, nchans entries or NULL */
+} gf_synth_desc;
+
+/* Generates time rows [t_begin, t_end) of the seeded observation defined in
+ * gaffa_b200/synth.py (same noise stream, bit for bit) into dev_out
+ * ([t_end - t_begin][row bytes]). */
+int gf_synth_generate(const gf_synth_desc* desc, uint64_t t_begin, uint64_t t_end,
+                      uint8_t* dev_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GAFFA_B200_H */

@@ -147,7 +147,9 @@ def plain_end_to_end(ref: Oracle) -> dict:
                               cfg.preprocess_options(), cfg.snr_threshold,
                               widths=np.array(cfg.width_trials, np.uint64))
     t2 = time.time()
-    tobs = dd.shape[1] * obs.tsamp
+    # observation length as the reference's pipeline driver passes it
+    # (cuda_dm_search_benchmark.cpp: header.tsamp * header.nsamples)
+    tobs = obs.nsamples * obs.tsamp
     cands = ref.select_candidates(peaks, tobs, cfg.frequency_cluster_radius,
                                   cfg.dm_cluster_radius)
     top = cands[0]

@@ -278,5 +278,5 @@ def test_port_matches_reference_plain_end_to_end(port, golden_plain):
                                widths=np.array(cfg.width_trials, np.uint64))
     assert len(peaks) == int(g["npeaks"])
     assert hashlib.sha256(peaks.tobytes()).hexdigest() == str(g["peaks_digest"])
-    cands = port.select_candidates(peaks, dd.shape[1] * obs.tsamp)
+    cands = port.select_candidates(peaks, obs.nsamples * obs.tsamp)
     assert np.array_equal(cands, g["candidates"])
