@@ -1,0 +1,355 @@
+#!/usr/bin/env python3
+"""Benchmark: DM-trial·samples/s of the full pulsar search on B200.
+
+One step = the whole search of one observation: stage the filterbank,
+dedisperse every DM trial, detrend + normalise, downsample per octave, FFA +
+boxcar S/N over every task, expand and sort peaks, select candidates and fold
+the best one.  `value` times steps whose filterbank is already resident in
+HBM; `e2e` times the same search through the public pipeline API from a
+pinned host filterbank (host->device copy inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gaffa|reference]
+
+Multi-GPU runs (torchrun) are replicas: every rank searches its own
+observation (weak scaling); time is the max over ranks.  `--impl reference`
+times the reference's own CPU implementation (compiled from its sources,
+oracle/_ref) on a bounded sample of DM trials of the same workload, on all
+host cores of rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DM-trial·samples/s searched"
+UNIT = "DM-trial·samples/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["gaffa", "reference"], default="gaffa")
+    ap.add_argument("--workload", default="survey_size")
+    ap.add_argument("--ndm", type=int, default=None, help="override the DM-trial count (testing)")
+    ap.add_argument("--nsamples-log2", type=int, default=None, help="override the length (testing)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU baseline sample time")
+    return ap.parse_args()
+
+
+def workload(args, rank: int = 0):
+    from gaffa_b200 import configs
+    kw = {}
+    if args.ndm:
+        kw["ndm"] = args.ndm
+    if args.nsamples_log2:
+        kw["nsamples"] = 1 << args.nsamples_log2
+    return configs.CONFIGS[args.workload](seed=rank, **kw)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.lines: list[str] = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_hbm_gbs():
+    try:
+        return float(json.loads(PEAKS_FILE.read_text())["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# Per-unit algorithmic bytes (one unit = one DM-trial x one output sample).
+def algorithmic_bytes(stage: str, cfg, ds, units: int) -> float:
+    obs = cfg.obs
+    if stage == "dedisperse":
+        # input read once + uint32 output written
+        in_bytes = obs.nsamples * obs.nchans * (1 if obs.nbits == 8 else 0.25)
+        return units * (4.0 + in_bytes / (cfg.ndm * ds.nout))
+    if stage == "preprocess":
+        return units * 8.0                    # uint32 in, float out, in place
+    if stage == "prepare":
+        return units * 4.0 + units / ds.nout * ds.ffa.prepared_floats * 4.0
+    if stage == "ffa":
+        # prepared block read once per task (rows*bins per task) per series
+        per_series = float(sum(int(t["rows"]) * int(t["bins"]) for t in ds.plan.tasks)) * 4.0
+        return units / ds.nout * per_series
+    return 0.0
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    """Reference CPU implementation (oracle/_ref, else the port) on a bounded
+    DM-trial sample of the workload, with every host core."""
+    import torch
+    if rank != 0:
+        return
+    from oracle.oracle import Oracle
+    kind = "reference" if Oracle.available("reference") else "port"
+    ref = Oracle(kind)
+    cfg = workload(args)
+    obs = cfg.obs
+    from gaffa_b200 import core
+    data = core.synth_generate(obs).cpu().numpy()
+    freq = obs.frequencies
+    nout = ref.output_nsamples(freq, obs.nsamples, cfg.dm_low, cfg.dm_step, cfg.ndm, obs.ref_frequency, obs.tsamp)
+    cores = os.cpu_count() or 1
+
+    def one_step(nsel):
+        idx = np.linspace(0, cfg.ndm - 1, nsel).round().astype(int)
+        t0 = time.perf_counter()
+        blocks = [ref.dedisperse_multi_dm(data, freq, cfg.dm_low + i * cfg.dm_step, cfg.dm_step, 1,
+                                          obs.ref_frequency, obs.tsamp)[:, :nout] for i in idx]
+        blk = np.ascontiguousarray(np.concatenate(blocks))
+        peaks = ref.find_dm_peaks(blk, cfg.dms[idx], obs.tsamp, cfg.plan_options(), cfg.preprocess_options(),
+                                  cfg.snr_threshold,
+                                  widths=None if cfg.width_trials is None else np.array(cfg.width_trials, np.uint64))
+        cands = ref.select_candidates(peaks, obs.nsamples * obs.tsamp)
+        if len(cands):
+            ref.fold(blk[0], float(cands[0]["period"]), obs.tsamp, cfg.fold_nbin)
+        return time.perf_counter() - t0
+
+    # size the sample: a small probe, then scale to the target seconds
+    probe = max(1, min(cfg.ndm, 2 * cores // 8 or 1))
+    dt = one_step(probe)
+    nsel = int(max(1, min(cfg.ndm, probe * args.cpu_seconds / max(dt, 1e-3))))
+    for _ in range(max(0, args.warmup - 1)):
+        one_step(nsel)
+    times = [one_step(nsel) for _ in range(args.steps)]
+    sec = sum(times) / len(times)
+    value = nsel * nout / sec
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
+        "config": {"workload": cfg.name, "nchans": obs.nchans, "nsamples": obs.nsamples, "ndm": cfg.ndm,
+                   "nout": nout, "dedispersion": cfg.dedispersion},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{nsel} of {cfg.ndm} DM trials (evenly spaced), full length, per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(cfg, host_input, seconds: float) -> dict:
+    from oracle.oracle import Oracle
+    kind = "reference" if Oracle.available("reference") else "port"
+    ref = Oracle(kind)
+    obs = cfg.obs
+    freq = obs.frequencies
+    data = host_input
+    nout = ref.output_nsamples(freq, obs.nsamples, cfg.dm_low, cfg.dm_step, cfg.ndm, obs.ref_frequency, obs.tsamp)
+
+    def run(nsel):
+        idx = np.linspace(0, cfg.ndm - 1, nsel).round().astype(int)
+        t0 = time.perf_counter()
+        blocks = [ref.dedisperse_multi_dm(data, freq, cfg.dm_low + i * cfg.dm_step, cfg.dm_step, 1,
+                                          obs.ref_frequency, obs.tsamp)[:, :nout] for i in idx]
+        blk = np.ascontiguousarray(np.concatenate(blocks))
+        peaks = ref.find_dm_peaks(blk, cfg.dms[idx], obs.tsamp, cfg.plan_options(), cfg.preprocess_options(),
+                                  cfg.snr_threshold,
+                                  widths=None if cfg.width_trials is None else np.array(cfg.width_trials, np.uint64))
+        ref.select_candidates(peaks, obs.nsamples * obs.tsamp)
+        return time.perf_counter() - t0
+
+    cores = os.cpu_count() or 1
+    probe = max(1, min(cfg.ndm, cores // 4 or 1))
+    dt = run(probe)
+    nsel = int(max(1, min(cfg.ndm, probe * seconds / max(dt, 1e-3))))
+    dt = run(nsel) if nsel != probe else dt
+    return {"value": nsel * nout / dt, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{nsel} of {cfg.ndm} DM trials (evenly spaced), full length: dedisperse_multi_dm_cpu + "
+                      f"find_dm_peaks_cpu + select_candidates_cpu, {dt:.1f} s"}
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    from gaffa_b200 import core, search
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    cfg = workload(args, rank)
+    obs = cfg.obs
+    raw = core.synth_generate(obs, device_id=local)          # device-resident filterbank
+    ds = search.from_config(cfg, device_id=local)
+    timers = {}
+
+    def step(src):
+        return ds.run(src, timers=timers)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(src, k):
+        timers.clear()
+        barrier()
+        torch.cuda.synchronize(device)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        res = None
+        for _ in range(k):
+            res = step(src)
+        b.record()
+        torch.cuda.synchronize(device)
+        barrier()
+        ms = a.elapsed_time(b) / k
+        if dist is not None:
+            t = torch.tensor([ms], device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, res
+
+    for _ in range(args.warmup):
+        step(raw)
+    with ClockSampler(local) as clk:
+        ms, res = timed(raw, args.steps)
+    stage_ms = {k: [s.elapsed_time(e) for s, e in v] for k, v in timers.items()}
+    clocks = clk.summary()
+    units = cfg.ndm * ds.nout
+    value = units * world / (ms / 1e3)
+
+    # roofline of the dominant stage
+    peak, peak_kind = measured_hbm_gbs()
+    totals = {k: sum(v) for k, v in stage_ms.items() if v}
+    dominant = max(totals, key=totals.get)
+    per_launch_ms = totals[dominant] / len(stage_ms[dominant])
+    launches_per_step = len(stage_ms[dominant]) / args.steps
+    units_per_launch = units / launches_per_step
+    alg = algorithmic_bytes(dominant, cfg, ds, units_per_launch)
+    achieved = alg / (per_launch_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": dominant, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_ms,
+                "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in totals.items()}}
+
+    e2e = None
+    host = None
+    if not args.no_e2e:
+        host = torch.empty(raw.shape, dtype=torch.uint8, pin_memory=True)
+        host.copy_(raw)
+        step(host)
+        ms_e2e, _ = timed(host, args.steps)
+        d2h = int(res.gpu_launches * 0) + len(res.peaks) * 24 + 16 + ds.fold_nbin * 12
+        e2e = {"value": units * world / (ms_e2e / 1e3), "unit": UNIT, "ms_per_step": ms_e2e,
+               "h2d_bytes_per_step": int(raw.numel()), "d2h_bytes_per_step": d2h}
+
+    baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        src = host.numpy() if host is not None else raw.cpu().numpy()
+        try:
+            baseline = cpu_baseline(cfg, src, args.cpu_seconds)
+        except Exception as exc:  # the baseline is reported, never the target
+            baseline = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                        "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": cfg.name, "nchans": obs.nchans, "nsamples": obs.nsamples, "nbits": obs.nbits,
+                       "ndm": cfg.ndm, "nout": ds.nout, "dedispersion": cfg.dedispersion,
+                       "ffa_tasks": ds.plan.task_count, "width_trials": list(ds.plan.width_trials),
+                       "dm_batch": ds.dm_batch, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (34 GB filterbank)", "peaks": len(res.peaks),
+                       "candidates": len(res.candidates)},
+            "e2e": e2e,
+            "gpu_launches": res.gpu_launches * args.steps,
+            "roofline": roofline,
+            "cpu_baseline": baseline,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -127,9 +127,9 @@ class DedispersionProgram:
         self.dm_low, self.dm_step, self.tsamp = dm_low, dm_step, tsamp
 
     def close(self):
-        if getattr(self, "_h", None):
-            _lib.lib().gf_dedisp_program_destroy(self._h)
-            self._h = None
+        h, self._h = getattr(self, "_h", None), None
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.gf_dedisp_program_destroy(h)
 
     __del__ = close
 
@@ -265,11 +265,13 @@ class FfaProgram:
         self.counters = torch.zeros(2, dtype=torch.int64, device=self.device)
         self.capacity = 1 << 16
         self.peaks = torch.empty(self.capacity * 24, dtype=torch.uint8, device=self.device)
+        rows = plan.tasks["rows"].astype(np.int64)
+        self._leaf_depths = np.ceil(np.log2(np.maximum(rows, 1) / 64.0)).clip(0)
 
     def close(self):
-        if getattr(self, "_h", None):
-            _lib.lib().gf_ffa_program_destroy(self._h)
-            self._h = None
+        h, self._h = getattr(self, "_h", None), None
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.gf_ffa_program_destroy(h)
 
     __del__ = close
 
@@ -291,26 +293,39 @@ class FfaProgram:
             check(_lib.lib().gf_ffa_search(self._h, ptr(prepared), nseries, snr_threshold, ptr(self.scratch),
                                            ptr(self.peaks), self.capacity, ptr(self.counters), _stream(stream)))
 
-    def search(self, prepared: torch.Tensor, nseries: int, snr_threshold: float = 6.0,
-               max_peaks: int = 0, stream=None) -> np.ndarray:
-        """Transform + detect every task of every series; returns the compact
-        peak records (PEAK_RECORD_DTYPE, unordered).  A peak buffer overflow
-        grows the buffer and re-runs, as CudaFfaTileRunner does
+    @property
+    def has_small(self) -> bool:
+        return bool(np.any(self._leaf_depths == 0))
+
+    @property
+    def has_big(self) -> bool:
+        return bool(np.any(self._leaf_depths > 0))
+
+    def collect(self, prepared: torch.Tensor, nseries: int, snr_threshold: float, max_peaks: int = 0,
+                stream=None) -> np.ndarray:
+        """Reads the records of the last search_async; on a peak-buffer
+        overflow grows the buffer and re-runs, as CudaFfaTileRunner does
         (ffa_cuda_executor.cuh:395-404,491-531)."""
-        if not math.isfinite(snr_threshold):
-            raise ValueError("FFA search S/N threshold must be finite")
         while True:
-            self.search_async(prepared, nseries, snr_threshold, stream)
-            counts = self.counters.cpu()
-            n = int(counts[0])
+            n = int(self.counters[0].item())
             if n <= self.capacity:
                 break
             self.capacity = int(n * 1.25) + 1024
             self.peaks = torch.empty(self.capacity * 24, dtype=torch.uint8, device=self.device)
+            self.search_async(prepared, nseries, snr_threshold, stream)
         if max_peaks and n > max_peaks * nseries:
             raise RuntimeError("FFA detection peak count exceeded max_peaks safety guard")
         raw = self.peaks[: n * 24].cpu().numpy()
         return raw.view(_lib.PEAK_RECORD_DTYPE).copy()
+
+    def search(self, prepared: torch.Tensor, nseries: int, snr_threshold: float = 6.0,
+               max_peaks: int = 0, stream=None) -> np.ndarray:
+        """Transform + detect every task of every series; returns the compact
+        peak records (PEAK_RECORD_DTYPE, unordered)."""
+        if not math.isfinite(snr_threshold):
+            raise ValueError("FFA search S/N threshold must be finite")
+        self.search_async(prepared, nseries, snr_threshold, stream)
+        return self.collect(prepared, nseries, snr_threshold, max_peaks, stream)
 
     def expand(self, records: np.ndarray, series_offset: int = 0, dm_low: float = 0.0,
                dm_step: float = 0.0) -> np.ndarray:

@@ -96,11 +96,17 @@ __global__ void __launch_bounds__(128) running_median_kernel(const void* __restr
     __syncwarp();
   }
   const int slots = cap / 32;
+  float pre_out = 0.0f, pre_in = 0.0f;
   for (uint64_t i = 0; i < n; ++i) {
     if (lane == 0) orow[i] = A[half];
     if (i + 1 == n) break;
-    const float x_out = padded(static_cast<int64_t>(i));
-    const float x_in = padded(static_cast<int64_t>(i) + w);
+    // every 32 steps each lane fetches one outgoing and one incoming value
+    if ((i & 31) == 0) {
+      pre_out = padded(static_cast<int64_t>(i) + lane);
+      pre_in = padded(static_cast<int64_t>(i) + w + lane);
+    }
+    const float x_out = __shfl_sync(0xffffffffu, pre_out, static_cast<int>(i & 31));
+    const float x_in = __shfl_sync(0xffffffffu, pre_in, static_cast<int>(i & 31));
     // position of the first copy of x_out, and rank of x_in
     int p = cap;
     int less = 0;
@@ -164,29 +170,61 @@ __global__ void __launch_bounds__(256) detrend_kernel(void* series, uint64_t str
   reinterpret_cast<float*>(row)[i] = __fsub_rn(x, trend);
 }
 
-// Sequential FP64 sums in the reference order, one thread per series.
-__global__ void __launch_bounds__(32) stats_kernel(const float* __restrict__ series, uint64_t stride, uint64_t n,
-                                                   int nseries, int normalise, int reject_constant,
-                                                   double* __restrict__ stats, uint32_t* status) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+// Sequential FP64 sums in the reference order, one warp per series: the
+// lanes stream the series into shared memory with cp.async (two chunks in
+// flight) while lane 0 runs the dependent chain sum += y; sq += y * y over the
+// chunk already resident, so the chain never waits on global memory.
+constexpr int kStatsChunk = 1024;  // floats per chunk
+constexpr int kStatsWarps = 4;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+__global__ void __launch_bounds__(32 * kStatsWarps) stats_kernel(const float* __restrict__ series, uint64_t stride,
+                                                                 uint64_t n, int nseries, int normalise,
+                                                                 int reject_constant, double* __restrict__ stats,
+                                                                 uint32_t* status) {
+  __shared__ __align__(16) float buf[kStatsWarps][2][kStatsChunk];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = blockIdx.x * kStatsWarps + warp;
   if (s >= nseries) return;
   const float* row = series + static_cast<uint64_t>(s) * stride;
-  double sum = 0.0, sq = 0.0;
-  uint64_t i = 0;
-  if ((reinterpret_cast<uintptr_t>(row) & 15) == 0) {
-    const float4* v = reinterpret_cast<const float4*>(row);
-    const uint64_t nv = n / 4;
-    for (uint64_t k = 0; k < nv; ++k) {
-      const float4 q = __ldg(v + k);
-      const double a = q.x, b = q.y, c = q.z, d = q.w;
-      sum = __dadd_rn(sum, a); sq = __dadd_rn(sq, __dmul_rn(a, a));
-      sum = __dadd_rn(sum, b); sq = __dadd_rn(sq, __dmul_rn(b, b));
-      sum = __dadd_rn(sum, c); sq = __dadd_rn(sq, __dmul_rn(c, c));
-      sum = __dadd_rn(sum, d); sq = __dadd_rn(sq, __dmul_rn(d, d));
+  // vector staging needs 16-byte aligned rows; others take the scalar tail path
+  const uint64_t nvec = (reinterpret_cast<uintptr_t>(row) & 15) == 0 ? n / 4 : 0;
+  const uint64_t nchunks = (nvec * 4 + kStatsChunk - 1) / kStatsChunk;
+  auto issue = [&](uint64_t c) {
+    if (c < nchunks) {
+      const uint64_t v0 = c * (kStatsChunk / 4);
+      for (int v = lane; v < kStatsChunk / 4; v += 32)
+        if (v0 + v < nvec) cp_async16(&buf[warp][c & 1][4 * v], row + 4 * (v0 + v));
     }
-    i = nv * 4;
+    cp_async_commit();
+  };
+  double sum = 0.0, sq = 0.0;
+  issue(0);
+  for (uint64_t c = 0; c < nchunks; ++c) {
+    issue(c + 1);
+    cp_async_wait_1();
+    __syncwarp();
+    if (lane == 0) {
+      const float* b = buf[warp][c & 1];
+      const uint64_t len = umin64(kStatsChunk, nvec * 4 - c * kStatsChunk);
+      for (uint64_t i = 0; i < len; ++i) {
+        const double a = b[i];
+        sum = __dadd_rn(sum, a);
+        sq = __dadd_rn(sq, __dmul_rn(a, a));
+      }
+    }
+    __syncwarp();
   }
-  for (; i < n; ++i) {
+  cp_async_wait_0();
+  if (lane != 0) return;
+  for (uint64_t i = nvec * 4; i < n; ++i) {
     const double a = row[i];
     sum = __dadd_rn(sum, a);
     sq = __dadd_rn(sq, __dmul_rn(a, a));
@@ -322,7 +360,7 @@ extern "C" int gf_preprocess_inplace(const gf_preprocess_desc* d, void* dev_seri
         detrend_kernel<false, false><<<dg, 256, 0, s>>>(dev_series, stride, n, lowmed, g.low_stride, g.low_n, g.factor, dev_status);
     }
     cuda_check(cudaGetLastError(), "detrend launch");
-    stats_kernel<<<static_cast<unsigned>(ceil_div(nseries, 32)), 32, 0, s>>>(
+    stats_kernel<<<static_cast<unsigned>(ceil_div(nseries, kStatsWarps)), 32 * kStatsWarps, 0, s>>>(
         static_cast<const float*>(dev_series), stride, n, static_cast<int>(nseries), d->normalise,
         d->reject_constant, dev_stats, dev_status);
     cuda_check(cudaGetLastError(), "stats launch");

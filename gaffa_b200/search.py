@@ -36,6 +36,25 @@ class SearchResult:
         return self.ndm * self.nout
 
 
+class _StageTimer:
+    """Records CUDA events around a stage's launches into timers[name]."""
+
+    def __init__(self, timers, name):
+        self.timers, self.name = timers, name
+
+    def __enter__(self):
+        if self.timers is not None:
+            self.a = torch.cuda.Event(enable_timing=True)
+            self.a.record()
+        return self
+
+    def __exit__(self, *exc):
+        if self.timers is not None:
+            b = torch.cuda.Event(enable_timing=True)
+            b.record()
+            self.timers.setdefault(self.name, []).append((self.a, b))
+
+
 class DmSearch:
     """A reusable search for one observation geometry and set of options."""
 
@@ -91,20 +110,29 @@ class DmSearch:
     def stage(self, filterbank) -> torch.Tensor:
         return self.dedisp.stage(filterbank)
 
-    def search_staged(self, staged: torch.Tensor, timings: dict | None = None) -> tuple:
-        """Runs every DM batch; returns (raw peaks, launches)."""
-        timings = {} if timings is None else timings
+    def search_staged(self, staged: torch.Tensor, timers: dict | None = None) -> tuple:
+        """Runs every DM batch; returns (raw peaks, kernel launches).
+
+        timers (optional) collects CUDA events around each stage's launches:
+        dedisperse, preprocess, prepare, ffa."""
         parts = []
         launches = 0
+        dd_kernels = 1 if self.dedisp.algorithm == "brute" else 2
+        ffa_kernels = int(self.ffa.has_small) + int(self.ffa.has_big)
         for b0 in range(0, self.ndm, self.dm_batch):
             cnt = min(self.dm_batch, self.ndm - b0)
-            dd = self.dedisp.run(staged, b0, cnt, out=self._series, out_stride=self.out_stride,
-                                 workspace=self._workspace)
-            stats = self.pre.run(dd, cnt)
-            self.ffa.prepare(dd.view(torch.float32), cnt, stats, out=self._prepared)
-            rec = self.ffa.search(self._prepared, cnt, self.snr_threshold)
+            with _StageTimer(timers, "dedisperse"):
+                dd = self.dedisp.run(staged, b0, cnt, out=self._series, out_stride=self.out_stride,
+                                     workspace=self._workspace)
+            with _StageTimer(timers, "preprocess"):
+                stats = self.pre.run(dd, cnt)
+            with _StageTimer(timers, "prepare"):
+                self.ffa.prepare(dd.view(torch.float32), cnt, stats, out=self._prepared)
+            with _StageTimer(timers, "ffa"):
+                self.ffa.search_async(self._prepared, cnt, self.snr_threshold)
+            rec = self.ffa.collect(self._prepared, cnt, self.snr_threshold)
             parts.append(self.ffa.expand(rec, b0, self.dm_low, self.dm_step))
-            launches += 1 + 4 + 1 + 2
+            launches += dd_kernels + 4 + 1 + ffa_kernels
         self.pre.synchronize()
         peaks = np.concatenate(parts) if parts else np.zeros(0, _lib.PEAK_DTYPE)
         return peaks, launches
@@ -121,13 +149,14 @@ class DmSearch:
         row = dd[dm_index - b0, : self.nout]
         return core.fold_time_series(row, period, self.tsamp, self.fold_nbin)
 
-    def run(self, filterbank, observation_seconds: float | None = None) -> SearchResult:
+    def run(self, filterbank, observation_seconds: float | None = None, timers: dict | None = None) -> SearchResult:
         t = {}
         t0 = time.perf_counter()
-        staged = self.stage(filterbank)
+        with _StageTimer(timers, "stage"):
+            staged = self.stage(filterbank)
         torch.cuda.synchronize(self.device)
         t1 = time.perf_counter()
-        peaks, launches = self.search_staged(staged, t)
+        peaks, launches = self.search_staged(staged, timers)
         t2 = time.perf_counter()
         peaks = core.sort_peaks(peaks)
         tobs = self.nsamples * self.tsamp if observation_seconds is None else observation_seconds
