@@ -24,6 +24,7 @@ GF_EOVERFLOW_PEAKS = -7
 STATUS_NONFINITE = 1
 STATUS_CONSTANT = 2
 STATUS_PEAK_OVERFLOW = 4
+STATUS_SCHEDULE = 8
 
 DEDISP_BRUTE = 0
 DEDISP_SUBBAND = 1
@@ -69,7 +70,7 @@ class PreprocessInfo(C.Structure):
 
 class FfaInfo(C.Structure):
     _fields_ = [("ntasks", u64), ("noctaves", u64), ("prepared_floats", u64), ("scratch_bytes", u64),
-                ("max_task_elements", u64), ("metadata_bytes", u64)]
+                ("max_task_elements", u64), ("metadata_bytes", u64), ("nclasses", u64)]
 
 
 class CandidateOptions(C.Structure):

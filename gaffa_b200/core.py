@@ -265,8 +265,6 @@ class FfaProgram:
         self.counters = torch.zeros(2, dtype=torch.int64, device=self.device)
         self.capacity = 1 << 16
         self.peaks = torch.empty(self.capacity * 24, dtype=torch.uint8, device=self.device)
-        rows = plan.tasks["rows"].astype(np.int64)
-        self._leaf_depths = np.ceil(np.log2(np.maximum(rows, 1) / 64.0)).clip(0)
 
     def close(self):
         h, self._h = getattr(self, "_h", None), None
@@ -294,12 +292,8 @@ class FfaProgram:
                                            ptr(self.peaks), self.capacity, ptr(self.counters), _stream(stream)))
 
     @property
-    def has_small(self) -> bool:
-        return bool(np.any(self._leaf_depths == 0))
-
-    @property
-    def has_big(self) -> bool:
-        return bool(np.any(self._leaf_depths > 0))
+    def kernel_launches(self) -> int:
+        return int(self.info.nclasses)
 
     def collect(self, prepared: torch.Tensor, nseries: int, snr_threshold: float, max_peaks: int = 0,
                 stream=None) -> np.ndarray:
@@ -307,7 +301,10 @@ class FfaProgram:
         overflow grows the buffer and re-runs, as CudaFfaTileRunner does
         (ffa_cuda_executor.cuh:395-404,491-531)."""
         while True:
-            n = int(self.counters[0].item())
+            counts = self.counters.cpu()
+            if int(counts[1]) & _lib.STATUS_SCHEDULE:
+                raise RuntimeError("FFA block schedule exceeded its shared-memory tile")
+            n = int(counts[0])
             if n <= self.capacity:
                 break
             self.capacity = int(n * 1.25) + 1024

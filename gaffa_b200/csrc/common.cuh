@@ -86,6 +86,10 @@ struct DeviceBlob {
   DeviceBlob() = default;
   DeviceBlob(const DeviceBlob&) = delete;
   DeviceBlob& operator=(const DeviceBlob&) = delete;
+  DeviceBlob(DeviceBlob&& o) noexcept : ptr(o.ptr), bytes(o.bytes), device(o.device) {
+    o.ptr = nullptr;
+    o.bytes = 0;
+  }
   ~DeviceBlob() { release(); }
   void release() {
     if (ptr) {

@@ -51,7 +51,7 @@ struct TaskDev {
   float inv_stdnoise;
   uint32_t ntrials;
   uint32_t trial_offset;
-  uint32_t leaf_depth;    // depth of the on-chip subtrees (0: whole task)
+  uint32_t split_depth;   // depth of the on-chip subtrees (0: whole task in one CTA)
   uint32_t max_width;
   uint32_t reserved;
 };
@@ -149,15 +149,27 @@ __global__ void __launch_bounds__(kThreads) prepare_kernel(const float* __restri
 }
 
 // ---------------------------------------------------------------------------
-// FFA tree helpers
+// FFA tree evaluation
 // ---------------------------------------------------------------------------
+//
+// A level of the tree is a list of rows, each produced by one MetaEntry:
+//   MERGE  out = prev[a] + roll_left(prev[b], roll mod bins)   (ffa.cpp:110-171)
+//   CARRY  out = prev[a]              (a one-row node carried up unchanged)
+//   LOAD   out = global row a         (input rows or rows of a lower pass)
+// Rows of a level live in one of two shared-memory buffers (pitch = bins|1);
+// levels alternate buffers, so each level costs one __syncthreads.
+
+enum : uint16_t { kMerge = 0, kCarry = 1, kLoad = 2 };
+
+struct MetaEntry {
+  uint16_t op, a, b, roll;
+};
 
 struct Node {
   uint32_t a, n, depth;
 };
 
-// The node at depth `depth` containing row r of an n-row tree, stopping early
-// at one-row nodes (their depth is then < `depth`).
+// The node at depth `depth` containing row r (stops at one-row nodes).
 __device__ __forceinline__ Node node_of(uint32_t r, uint32_t n, uint32_t depth) {
   Node nd{0u, n, 0u};
   while (nd.depth < depth && nd.n > 1) {
@@ -173,77 +185,76 @@ __device__ __forceinline__ Node node_of(uint32_t r, uint32_t n, uint32_t depth) 
   return nd;
 }
 
-struct MergeIdx {
-  uint32_t head_row, tail_row, roll;
-  bool head_leaf, tail_leaf;
-};
-
-// ffa.cpp:153-171 merge_row index arithmetic for output row s of node (a, n)
-__device__ __forceinline__ MergeIdx merge_index(uint32_t a, uint32_t n, uint32_t s, uint32_t bins) {
-  const uint32_t h = n >> 1, t = n - h;
-  const float nm1 = static_cast<float>(n - 1);
-  const float hsc = __fdiv_rn(static_cast<float>(h - 1), nm1);
-  const float tsc = __fdiv_rn(static_cast<float>(t - 1), nm1);
-  const uint32_t hs = static_cast<uint32_t>(__fadd_rn(__fmul_rn(hsc, static_cast<float>(s)), 0.5f));
-  const uint32_t ts = static_cast<uint32_t>(__fadd_rn(__fmul_rn(tsc, static_cast<float>(s)), 0.5f));
-  MergeIdx m;
-  m.head_row = a + hs;
-  m.tail_row = a + h + ts;
-  m.roll = (s - ts) % bins;
-  m.head_leaf = h == 1;
-  m.tail_leaf = t == 1;
-  return m;
-}
-
-// out[j] = head[j] + tail[(j + roll) mod bins] for one row, by one warp
-__device__ __forceinline__ void merge_row_warp(const float* __restrict__ head, const float* __restrict__ tail,
-                                               uint32_t roll, uint32_t bins, float* __restrict__ out, int lane) {
-  for (uint32_t j = lane; j < bins; j += 32) {
-    uint32_t k = j + roll;
-    if (k >= bins) k -= bins;
-    out[j] = __fadd_rn(head[j], tail[k]);
-  }
-}
-
-__device__ __forceinline__ void merge_row_warp_global(const float* head, const float* tail, uint32_t roll,
-                                                      uint32_t bins, float* out, int lane) {
-  for (uint32_t j = lane; j < bins; j += 32) {
-    uint32_t k = j + roll;
-    if (k >= bins) k -= bins;
-    __stcg(out + j, __fadd_rn(__ldcg(head + j), __ldcg(tail + k)));
-  }
-}
-
-// Transforms the subtree rooted at node (a0, n0) (depth d0 of an n-row tree)
-// on chip, for depths from the deepest up to `stop_depth` inclusive.  Input
-// rows come from `input` (global); node outputs of depth d live in
-// buf[d & 1] at row index (row - a0).  Returns nothing; callers read
-// buf[stop_depth & 1].
-__device__ void transform_subtree(const float* __restrict__ input, uint32_t nrows, uint32_t bins, uint32_t a0,
-                                  uint32_t n0, uint32_t d0, uint32_t stop_depth, float* buf0, float* buf1,
-                                  uint32_t pitch) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // deepest depth with a split inside the subtree
-  uint32_t max_d = d0;
-  {
-    uint32_t n = n0;
-    while (n > 1) { n = (n + 1) >> 1; ++max_d; }
-  }
-  for (int d = static_cast<int>(max_d) - 1; d >= static_cast<int>(stop_depth); --d) {
-    float* out = (d & 1) ? buf1 : buf0;
-    const float* prev = (d & 1) ? buf0 : buf1;
-    for (uint32_t r = warp; r < n0; r += kThreads / 32) {
-      const Node nd = node_of(a0 + r, nrows, static_cast<uint32_t>(d));
-      if (nd.depth != static_cast<uint32_t>(d) || nd.n < 2) continue;
-      const MergeIdx m = merge_index(nd.a, nd.n, a0 + r - nd.a, bins);
-      const float* head = m.head_leaf ? input + static_cast<uint64_t>(m.head_row) * bins
-                                      : prev + (m.head_row - a0) * pitch;
-      const float* tail = m.tail_leaf ? input + static_cast<uint64_t>(m.tail_row) * bins
-                                      : prev + (m.tail_row - a0) * pitch;
-      merge_row_warp(head, tail, m.roll, bins, out + r * pitch, lane);
+// Node `index` (bits read MSB first, 0 = head) at depth `depth`.
+__device__ __forceinline__ Node node_at(uint32_t index, uint32_t n, uint32_t depth) {
+  Node nd{0u, n, depth};
+  for (uint32_t b = depth; b-- > 0;) {
+    const uint32_t h = nd.n >> 1;
+    if ((index >> b) & 1u) {
+      nd.a += h;
+      nd.n -= h;
+    } else {
+      nd.n = h;
     }
-    __syncthreads();
   }
+  return nd;
+}
+
+// ffa.cpp:153-171: hs = (size_t)(float((h-1)/(n-1)) * s + 0.5f), likewise ts
+__device__ __forceinline__ float shift_scale(uint32_t part, uint32_t n) {
+  return __fdiv_rn(static_cast<float>(part - 1), static_cast<float>(n - 1));
+}
+__device__ __forceinline__ uint32_t scaled_shift(float scale, uint32_t s) {
+  return static_cast<uint32_t>(__fadd_rn(__fmul_rn(scale, static_cast<float>(s)), 0.5f));
+}
+
+template <bool GlobalCg>
+__device__ __forceinline__ void eval_level(const MetaEntry* __restrict__ meta, uint32_t nrows,
+                                           const float* __restrict__ prev, float* __restrict__ out,
+                                           uint32_t pitch, const float* __restrict__ gsrc, uint32_t bins) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t q = warp; q < nrows; q += kThreads / 32) {
+    const MetaEntry m = meta[q];
+    float* o = out + q * pitch;
+    if (m.op == kMerge) {
+      const float* h = prev + m.a * pitch;
+      const float* t = prev + m.b * pitch;
+      const uint32_t r = m.roll < bins ? m.roll : m.roll % bins;
+      for (uint32_t j = lane; j < bins; j += 32) {
+        uint32_t k = j + r;
+        if (k >= bins) k -= bins;
+        o[j] = __fadd_rn(h[j], t[k]);
+      }
+    } else if (m.op == kCarry) {
+      const float* h = prev + m.a * pitch;
+      for (uint32_t j = lane; j < bins; j += 32) o[j] = h[j];
+    } else {
+      const float* g = gsrc + static_cast<uint64_t>(m.a) * bins;
+      for (uint32_t j = lane; j < bins; j += 32) o[j] = GlobalCg ? __ldcg(g + j) : __ldg(g + j);
+    }
+  }
+}
+
+// rows [0, n) of `src` (global, pitch bins, row a0 first) into smem
+template <bool GlobalCg>
+__device__ __forceinline__ void load_rows(const float* src, uint32_t n, uint32_t bins, float* out, uint32_t pitch) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t q = warp; q < n; q += kThreads / 32)
+    for (uint32_t j = lane; j < bins; j += 32)
+      out[q * pitch + j] = GlobalCg ? __ldcg(src + static_cast<uint64_t>(q) * bins + j)
+                                    : __ldg(src + static_cast<uint64_t>(q) * bins + j);
+}
+
+__device__ __forceinline__ void store_rows(const float* in, uint32_t pitch, uint32_t n, uint32_t bins, float* dst) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t q = warp; q < n; q += kThreads / 32)
+    for (uint32_t j = lane; j < bins; j += 32) __stcg(dst + static_cast<uint64_t>(q) * bins + j, in[q * pitch + j]);
+}
+
+__device__ __forceinline__ uint32_t tree_depth(uint32_t n) {
+  uint32_t d = 0;
+  while (n > 1) { n = (n + 1) >> 1; ++d; }
+  return d;
 }
 
 // ---------------------------------------------------------------------------
@@ -262,7 +273,8 @@ struct DetectArgs {
 
 // rows[i] (pitch `pitch`) hold root rows shift0 + i, i < count.  Prefix sums
 // are sequential per row (one thread per row, ffa_detection.cpp:126-139);
-// each warp then scans one row for every width.
+// each warp then scans one row for every width (first phase of the maximum,
+// :141-170) and appends peaks with S/N >= threshold.
 __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, uint32_t shift0, float* cp,
                             uint32_t cp_pitch, const DetectArgs& a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -330,6 +342,8 @@ struct SearchParams {
   uint64_t prep_stride;
   const TaskDev* tasks;
   const TrialDev* trials;
+  const MetaEntry* sub_meta;    // subtree schedules by size
+  const uint32_t* sub_offset;   // [max_rows + 1]
   const uint32_t* item_tasks;   // task indices of this launch's class
   uint32_t nitem_tasks;
   uint32_t nseries;
@@ -339,54 +353,13 @@ struct SearchParams {
   unsigned long long* counters;
   float* scratch;               // per cluster: 2 * scratch_elems floats
   uint64_t scratch_elems;
-  uint32_t max_bins;
-  uint32_t smem_pitch;          // pitch the shared buffers were sized with
+  uint32_t pitch;               // shared-memory row pitch (max bins | 1)
+  uint32_t max_rows;            // rows per shared-memory buffer
+  uint32_t block_rows;          // R: output rows per column block
+  uint32_t final_rows;          // R for the root pass (room for prefix sums)
+  uint32_t levels;              // K: levels per column pass
+  uint32_t* error;              // set when a schedule would overflow a buffer
 };
-
-__device__ __forceinline__ uint32_t pitch_of(uint32_t bins) { return bins | 1u; }
-
-// Detect the root rows [r0, r1) of a task whose root children are in
-// `child` (smem or global scratch, pitch cpitch) or are input rows.
-// rowbuf points at `avail` free floats of shared memory; the batch size is the
-// number of (row, prefix) pairs that fit.
-template <bool GlobalChildren>
-__device__ void root_detect(const float* input, const float* child, uint32_t cpitch, uint32_t nrows,
-                            uint32_t r0, uint32_t r1, float* rowbuf, uint32_t avail, const DetectArgs& da) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t bins = da.bins;
-  const uint32_t pitch = pitch_of(bins);
-  const uint32_t cp_pitch = (bins + da.max_width + 2) | 1u;
-  const uint32_t batch = umin32(kThreads, avail / (pitch + cp_pitch));
-  float* cp = rowbuf + batch * pitch;
-  for (uint32_t b0 = r0; b0 < r1; b0 += batch) {
-    const uint32_t cnt = umin32(batch, r1 - b0);
-    for (uint32_t i = warp; i < cnt; i += kThreads / 32) {
-      const uint32_t s = b0 + i;
-      if (nrows == 1) {
-        for (uint32_t j = lane; j < bins; j += 32) rowbuf[i * pitch + j] = input[j];
-        continue;
-      }
-      const MergeIdx m = merge_index(0, nrows, s, bins);
-      const float* head = m.head_leaf ? input + static_cast<uint64_t>(m.head_row) * bins
-                                      : child + static_cast<uint64_t>(m.head_row) * cpitch;
-      const float* tail = m.tail_leaf ? input + static_cast<uint64_t>(m.tail_row) * bins
-                                      : child + static_cast<uint64_t>(m.tail_row) * cpitch;
-      if (GlobalChildren) {
-        for (uint32_t j = lane; j < bins; j += 32) {
-          uint32_t k = j + m.roll;
-          if (k >= bins) k -= bins;
-          const float hv = m.head_leaf ? head[j] : __ldcg(head + j);
-          const float tv = m.tail_leaf ? tail[k] : __ldcg(tail + k);
-          rowbuf[i * pitch + j] = __fadd_rn(hv, tv);
-        }
-      } else {
-        merge_row_warp(head, tail, m.roll, bins, rowbuf + i * pitch, lane);
-      }
-    }
-    __syncthreads();
-    detect_rows(rowbuf, pitch, cnt, b0, cp, cp_pitch, da);
-  }
-}
 
 __device__ __forceinline__ DetectArgs make_detect(const SearchParams& p, const TaskDev& t, uint32_t series,
                                                   uint32_t task) {
@@ -405,90 +378,235 @@ __device__ __forceinline__ DetectArgs make_detect(const SearchParams& p, const T
   return da;
 }
 
-// One CTA per (series, task): the whole tree on chip.
-__global__ void __launch_bounds__(kThreads) ffa_small_kernel(SearchParams p) {
-  extern __shared__ float sm[];
-  const uint64_t nitems = static_cast<uint64_t>(p.nseries) * p.nitem_tasks;
-  for (uint64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const uint32_t series = static_cast<uint32_t>(item / p.nitem_tasks);
-    const uint32_t task = p.item_tasks[item % p.nitem_tasks];
-    const TaskDev t = p.tasks[task];
-    const float* input = p.prepared + series * p.prep_stride + t.prep_offset;
-    const uint32_t pitch = pitch_of(t.bins);
-    float* buf0 = sm;
-    float* buf1 = sm + kLeafRows * pitch;
-    // everything below the root
-    transform_subtree(input, t.rows, t.bins, 0, t.rows, 0, 1, buf0, buf1, pitch);
-    // root children are in buf1 (depth 1); the root rows go to detection in
-    // batches held in buf0, which depth 1 does not use.
-    const DetectArgs da = make_detect(p, t, series, task);
-    root_detect<false>(input, buf1, pitch, t.rows, 0, t.rows_eval, buf0, kLeafRows * pitch, da);
+// Evaluates a whole subtree of n <= max_rows rows starting at input row
+// `a` (pointer `src` = row a), from its input rows up to relative level
+// `stop` (0: the subtree root).  Returns the buffer holding level `stop`.
+__device__ float* eval_subtree(const SearchParams& p, const float* src, uint32_t n, uint32_t bins, uint32_t stop,
+                               float* buf0, float* buf1) {
+  const uint32_t pitch = p.pitch;
+  const uint32_t md = tree_depth(n);
+  float* bufs[2] = {buf0, buf1};
+  load_rows<false>(src, n, bins, bufs[md & 1], pitch);
+  __syncthreads();
+  const MetaEntry* table = p.sub_meta + p.sub_offset[n];
+  for (int l = static_cast<int>(md) - 1; l >= static_cast<int>(stop); --l) {
+    eval_level<false>(table + (md - 1 - l) * n, n, bufs[(l + 1) & 1], bufs[l & 1], pitch, nullptr, bins);
+    __syncthreads();
+  }
+  return bufs[stop & 1];
+}
+
+// Column block: rows [s0, s1) of node X (task rows, depth dx) computed from
+// the rows of depth dx + K held in global `src` (task row coordinates).
+// Warp 0 builds the per-level row schedules top-down (only the rows the
+// block needs, ffa.cpp index arithmetic); all warps then evaluate bottom-up.
+// The result (s1 - s0 rows) is in buf0.
+__device__ void eval_column(const SearchParams& p, Node X, uint32_t s0, uint32_t s1, uint32_t K, const float* src,
+                            uint32_t bins, float* buf0, float* buf1, MetaEntry* cmeta, uint32_t* counts) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t max_rows = p.max_rows;
+  if (warp == 0) {
+    // per level: up to 2^k nodes (K <= 3 -> <= 8), one per lane
+    uint32_t na = 0, nn = 0, nu0 = 0, nu1 = 0, noff = 0;  // this lane's node at the current level
+    uint32_t count = 1;
+    if (lane == 0) { na = X.a; nn = X.n; nu0 = s0; nu1 = s1; noff = 0; }
+    uint32_t rows = s1 - s0;
+    bool overflow = rows > max_rows;
+    for (uint32_t k = 0; k < K; ++k) {
+      // children of this lane's node
+      uint32_t ha = 0, hn = 0, hu0 = 0, hu1 = 0, ta = 0, tn = 0, tu0 = 0, tu1 = 0;
+      float hsc = 0.0f, tsc = 0.0f;
+      if (lane < count) {
+        const uint32_t h = nn >> 1, t = nn - h;
+        hsc = shift_scale(h, nn);
+        tsc = shift_scale(t, nn);
+        ha = na; hn = h; hu0 = scaled_shift(hsc, nu0); hu1 = scaled_shift(hsc, nu1 - 1) + 1;
+        ta = na + h; tn = t; tu0 = scaled_shift(tsc, nu0); tu1 = scaled_shift(tsc, nu1 - 1) + 1;
+      }
+      // offsets of the children rows at level k+1 (exclusive scan, head then tail)
+      const uint32_t len = (hu1 - hu0) + (tu1 - tu0);
+      uint32_t incl = len;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += v;
+      }
+      const uint32_t hoff = incl - len, toff = hoff + (hu1 - hu0);
+      const uint32_t next_rows = __shfl_sync(0xffffffffu, incl, 31);
+      overflow |= next_rows > max_rows;
+      if (lane == 0) counts[k + 1] = next_rows;
+      // schedule of level k: rows of each node, lanes over rows
+      MetaEntry* mk = cmeta + k * max_rows;
+      for (uint32_t i = 0; i < count; ++i) {
+        const uint32_t bu0 = __shfl_sync(0xffffffffu, nu0, i), bu1 = __shfl_sync(0xffffffffu, nu1, i);
+        const uint32_t boff = __shfl_sync(0xffffffffu, noff, i);
+        const float bh = __shfl_sync(0xffffffffu, hsc, i), bt = __shfl_sync(0xffffffffu, tsc, i);
+        const uint32_t bho = __shfl_sync(0xffffffffu, hoff, i), bto = __shfl_sync(0xffffffffu, toff, i);
+        const uint32_t bhu0 = __shfl_sync(0xffffffffu, hu0, i), btu0 = __shfl_sync(0xffffffffu, tu0, i);
+        for (uint32_t u = bu0 + lane; u < bu1 && !overflow; u += 32) {
+          const uint32_t hs = scaled_shift(bh, u), ts = scaled_shift(bt, u);
+          MetaEntry m;
+          m.op = kMerge;
+          m.a = static_cast<uint16_t>(bho + hs - bhu0);
+          m.b = static_cast<uint16_t>(bto + ts - btu0);
+          m.roll = static_cast<uint16_t>(u - ts);
+          mk[boff + u - bu0] = m;
+        }
+      }
+      // children become the nodes of level k+1: lane l takes child l
+      const uint32_t src_lane = lane >> 1;
+      const bool is_tail = lane & 1;
+      const uint32_t c_ha = __shfl_sync(0xffffffffu, ha, src_lane), c_ta = __shfl_sync(0xffffffffu, ta, src_lane);
+      const uint32_t c_hn = __shfl_sync(0xffffffffu, hn, src_lane), c_tn = __shfl_sync(0xffffffffu, tn, src_lane);
+      const uint32_t c_hu0 = __shfl_sync(0xffffffffu, hu0, src_lane), c_tu0 = __shfl_sync(0xffffffffu, tu0, src_lane);
+      const uint32_t c_hu1 = __shfl_sync(0xffffffffu, hu1, src_lane), c_tu1 = __shfl_sync(0xffffffffu, tu1, src_lane);
+      const uint32_t c_ho = __shfl_sync(0xffffffffu, hoff, src_lane), c_to = __shfl_sync(0xffffffffu, toff, src_lane);
+      na = is_tail ? c_ta : c_ha;
+      nn = is_tail ? c_tn : c_hn;
+      nu0 = is_tail ? c_tu0 : c_hu0;
+      nu1 = is_tail ? c_tu1 : c_hu1;
+      noff = is_tail ? c_to : c_ho;
+      count *= 2;
+      rows = next_rows;
+    }
+    // bottom level K: rows loaded from src
+    MetaEntry* mK = cmeta + K * max_rows;
+    for (uint32_t i = 0; i < count; ++i) {
+      const uint32_t ba = __shfl_sync(0xffffffffu, na, i);
+      const uint32_t bu0 = __shfl_sync(0xffffffffu, nu0, i), bu1 = __shfl_sync(0xffffffffu, nu1, i);
+      const uint32_t boff = __shfl_sync(0xffffffffu, noff, i);
+      for (uint32_t u = bu0 + lane; u < bu1 && !overflow; u += 32) {
+        MetaEntry m;
+        m.op = kLoad;
+        m.a = static_cast<uint16_t>(ba + u);
+        m.b = 0;
+        m.roll = 0;
+        mK[boff + u - bu0] = m;
+      }
+    }
+    if (lane == 0) {
+      counts[0] = s1 - s0;
+      if (overflow) {
+        for (uint32_t k = 0; k <= K; ++k) counts[k] = 0u;
+        atomicOr(p.error, GF_STATUS_SCHEDULE);
+      }
+    }
+  }
+  __syncthreads();
+  float* bufs[2] = {buf0, buf1};
+  // a failed schedule leaves counts at 0: nothing is evaluated
+  eval_level<true>(cmeta + K * max_rows, counts[K], nullptr, bufs[K & 1], p.pitch, src, bins);
+  __syncthreads();
+  for (int k = static_cast<int>(K) - 1; k >= 0; --k) {
+    eval_level<false>(cmeta + k * max_rows, counts[k], bufs[(k + 1) & 1], bufs[k & 1], p.pitch, nullptr, bins);
+    __syncthreads();
   }
 }
 
-// A cluster of kClusterSize CTAs per (series, task) for tasks larger than a
-// CTA.  Scratch (global, per cluster) holds two full task buffers.
-__global__ void __cluster_dims__(kClusterSize, 1, 1) __launch_bounds__(kThreads)
-    ffa_cluster_kernel(SearchParams p) {
-  extern __shared__ float sm[];
+// Pass boundaries: depth cuts from split_depth down to 0, final pass K levels
+// (or fewer), earlier passes K levels, the remainder at the bottom.
+__device__ __forceinline__ uint32_t cut_after(uint32_t d, uint32_t dS, uint32_t K) {
+  // next (shallower) cut below depth d in the chain dS -> ... -> 0
+  const uint32_t r = dS % K;
+  if (d == dS && r != 0) return dS - r;
+  return d >= K ? d - K : 0;
+}
+
+// One (series, task) per cluster (cluster size 1, 2, 4 or 8).
+__global__ void __launch_bounds__(kThreads, 2) ffa_task_kernel(SearchParams p) {
+  extern __shared__ __align__(16) float sm[];
   cg::cluster_group cluster = cg::this_cluster();
+  const uint32_t cs = cluster.num_blocks();
   const uint32_t rank = cluster.block_rank();
-  const uint32_t cid = blockIdx.x / kClusterSize;
-  const uint32_t nclusters = gridDim.x / kClusterSize;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* q0 = p.scratch + static_cast<uint64_t>(cid) * 2 * p.scratch_elems;
-  float* q1 = q0 + p.scratch_elems;
+  const uint32_t cid = blockIdx.x / cs;
+  const uint32_t nclusters = gridDim.x / cs;
+  const uint32_t pitch = p.pitch;
+  float* buf0 = sm;
+  float* buf1 = sm + p.max_rows * pitch;
+  MetaEntry* cmeta = reinterpret_cast<MetaEntry*>(buf1 + p.max_rows * pitch);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(cmeta + (p.levels + 1) * p.max_rows);
+  float* q0 = p.scratch ? p.scratch + static_cast<uint64_t>(cid) * 2 * p.scratch_elems : nullptr;
+  float* q1 = q0 ? q0 + p.scratch_elems : nullptr;
   const uint64_t nitems = static_cast<uint64_t>(p.nseries) * p.nitem_tasks;
   for (uint64_t item = cid; item < nitems; item += nclusters) {
     const uint32_t series = static_cast<uint32_t>(item / p.nitem_tasks);
     const uint32_t task = p.item_tasks[item % p.nitem_tasks];
     const TaskDev t = p.tasks[task];
     const float* input = p.prepared + series * p.prep_stride + t.prep_offset;
-    const uint32_t bins = t.bins, pitch = pitch_of(bins);
-    const uint32_t dl = t.leaf_depth;
-    float* buf0 = sm;
-    float* buf1 = sm + kLeafRows * pitch;
-    // 1. subtrees at depth dl, on chip, written to scratch[dl & 1]
-    const uint32_t nleaves = 1u << dl;
-    float* qdl = (dl & 1) ? q1 : q0;
-    for (uint32_t leaf = rank; leaf < nleaves; leaf += kClusterSize) {
-      // locate leaf `leaf` (bits MSB first)
-      uint32_t a = 0, n = t.rows;
-      for (uint32_t b = dl; b-- > 0;) {
-        const uint32_t h = n >> 1;
-        if ((leaf >> b) & 1u) { a += h; n -= h; } else { n = h; }
+    const uint32_t bins = t.bins;
+    const DetectArgs da = make_detect(p, t, series, task);
+    const uint32_t cp_pitch = (bins + t.max_width + 2) | 1u;
+    const uint32_t dS = t.split_depth;
+    if (dS == 0) {
+      // whole task on chip: levels below the root, then root rows in batches
+      if (t.rows == 1) {
+        load_rows<false>(input, 1, bins, buf0, pitch);
+        __syncthreads();
+        detect_rows(buf0, pitch, 1, 0, buf1, cp_pitch, da);
+        continue;
       }
-      if (n > 1) transform_subtree(input, t.rows, bins, a, n, dl, dl, buf0, buf1, pitch);
-      const float* src = (n > 1) ? ((dl & 1) ? buf1 : buf0) : nullptr;
-      for (uint32_t r = warp; r < n; r += kThreads / 32)
-        for (uint32_t j = lane; j < bins; j += 32)
-          __stcg(qdl + static_cast<uint64_t>(a + r) * bins + j,
-                 src ? src[r * pitch + j] : input[static_cast<uint64_t>(a + r) * bins + j]);
+      float* lvl1 = eval_subtree(p, input, t.rows, bins, 1, buf0, buf1);
+      float* other = lvl1 == buf0 ? buf1 : buf0;
+      const uint32_t md = tree_depth(t.rows);
+      const MetaEntry* root = p.sub_meta + p.sub_offset[t.rows] + (md - 1) * t.rows;
+      const uint32_t batch = umin32(kThreads, (p.max_rows * pitch) / (pitch + cp_pitch));
+      for (uint32_t b0 = 0; b0 < t.rows_eval; b0 += batch) {
+        const uint32_t cnt = umin32(batch, t.rows_eval - b0);
+        eval_level<false>(root + b0, cnt, lvl1, other, pitch, nullptr, bins);
+        __syncthreads();
+        detect_rows(other, pitch, cnt, b0, other + batch * pitch, cp_pitch, da);
+      }
+      continue;
+    }
+    // 1. subtrees at depth dS, on chip, into scratch q0
+    const uint32_t nsub = 1u << dS;
+    for (uint32_t sub = rank; sub < nsub; sub += cs) {
+      const Node nd = node_at(sub, t.rows, dS);
+      if (nd.n == 1) {
+        load_rows<false>(input + static_cast<uint64_t>(nd.a) * bins, 1, bins, buf0, pitch);
+        __syncthreads();
+        store_rows(buf0, pitch, 1, bins, q0 + static_cast<uint64_t>(nd.a) * bins);
+      } else {
+        const float* res = eval_subtree(p, input + static_cast<uint64_t>(nd.a) * bins, nd.n, bins, 0, buf0, buf1);
+        store_rows(res, pitch, nd.n, bins, q0 + static_cast<uint64_t>(nd.a) * bins);
+      }
       __syncthreads();
     }
     cluster.sync();
-    // 2. depths dl-1 .. 1 through scratch, rows split across the cluster
-    const uint32_t rows_per = (t.rows + kClusterSize - 1) / kClusterSize;
-    const uint32_t r0 = rank * rows_per, r1 = min(t.rows, r0 + rows_per);
-    for (int d = static_cast<int>(dl) - 1; d >= 1; --d) {
-      float* out = (d & 1) ? q1 : q0;
-      const float* prev = (d & 1) ? q0 : q1;
-      for (uint32_t r = r0 + warp; r < r1; r += kThreads / 32) {
-        const Node nd = node_of(r, t.rows, static_cast<uint32_t>(d));
-        const MergeIdx m = merge_index(nd.a, nd.n, r - nd.a, bins);
-        merge_row_warp_global(prev + static_cast<uint64_t>(m.head_row) * bins,
-                              prev + static_cast<uint64_t>(m.tail_row) * bins, m.roll, bins,
-                              out + static_cast<uint64_t>(r) * bins, lane);
+    // 2. column passes up to the root
+    float* src = q0;
+    float* dst = q1;
+    uint32_t d = dS;
+    while (true) {
+      const uint32_t dn = cut_after(d, dS, p.levels);
+      const uint32_t K = d - dn;
+      const bool final_pass = dn == 0;
+      const uint32_t R = final_pass ? p.final_rows : p.block_rows;
+      const uint32_t nnodes = 1u << dn;
+      const uint32_t maxn = (t.rows + nnodes - 1) >> dn;
+      const uint32_t limit = final_pass ? t.rows_eval : maxn;
+      const uint32_t bpn = (limit + R - 1) / R;
+      const uint32_t units = nnodes * bpn;
+      for (uint32_t u = rank; u < units; u += cs) {
+        const Node X = node_at(u / bpn, t.rows, dn);
+        const uint32_t s0 = (u % bpn) * R;
+        const uint32_t s1 = umin32(s0 + R, final_pass ? t.rows_eval : X.n);
+        if (s0 >= s1) continue;
+        eval_column(p, X, s0, s1, K, src, bins, buf0, buf1, cmeta, counts);
+        if (final_pass) {
+          detect_rows(buf0, pitch, counts[0], s0, buf1, cp_pitch, da);
+        } else {
+          store_rows(buf0, pitch, counts[0], bins, dst + static_cast<uint64_t>(X.a + s0) * bins);
+          __syncthreads();
+        }
       }
       cluster.sync();
+      if (final_pass) break;
+      float* tmp = src;
+      src = dst;
+      dst = tmp;
+      d = dn;
     }
-    // 3. root rows [0, rows_eval) split across the cluster, fused detection
-    const DetectArgs da = make_detect(p, t, series, task);
-    const uint32_t ev_per = (t.rows_eval + kClusterSize - 1) / kClusterSize;
-    const uint32_t e0 = min(t.rows_eval, rank * ev_per), e1 = min(t.rows_eval, e0 + ev_per);
-    root_detect<true>(input, q1, bins, t.rows, e0, e1, sm, 2 * kLeafRows * p.smem_pitch, da);
-    // scratch is reused by the next item
-    cluster.sync();
   }
 }
 
@@ -506,18 +624,32 @@ __global__ void __launch_bounds__(kThreads) ffa_level_kernel(const float* __rest
       out[static_cast<uint64_t>(r) * bins + j] = input[static_cast<uint64_t>(r) * bins + j];
     return;
   }
-  const MergeIdx m = merge_index(nd.a, nd.n, r - nd.a, bins);
-  const float* head = m.head_leaf ? input + static_cast<uint64_t>(m.head_row) * bins
-                                  : prev + static_cast<uint64_t>(m.head_row) * bins;
-  const float* tail = m.tail_leaf ? input + static_cast<uint64_t>(m.tail_row) * bins
-                                  : prev + static_cast<uint64_t>(m.tail_row) * bins;
-  merge_row_warp(head, tail, m.roll, bins, out + static_cast<uint64_t>(r) * bins, lane);
+  const uint32_t h = nd.n >> 1, t = nd.n - h;
+  const uint32_t s = r - nd.a;
+  const uint32_t hs = scaled_shift(shift_scale(h, nd.n), s), ts = scaled_shift(shift_scale(t, nd.n), s);
+  const float* head = (h == 1 ? input : prev) + static_cast<uint64_t>(nd.a + hs) * bins;
+  const float* tail = (t == 1 ? input : prev) + static_cast<uint64_t>(nd.a + h + ts) * bins;
+  const uint32_t roll = (s - ts) % bins;
+  for (uint32_t j = lane; j < bins; j += 32) {
+    uint32_t k = j + roll;
+    if (k >= bins) k -= bins;
+    out[static_cast<uint64_t>(r) * bins + j] = __fadd_rn(head[j], tail[k]);
+  }
 }
 
 }  // namespace
 }  // namespace gf
 
 using namespace gf;
+
+struct FfaClass {
+  int cluster = 1;             // CTAs cooperating on one (series, task)
+  std::vector<uint32_t> tasks;
+  uint64_t max_elems = 0;      // rows * bins of the largest task (scratch per cluster)
+  int nclusters = 0;           // resident clusters
+  uint64_t scratch_offset = 0; // floats into the program scratch
+  DeviceBlob tasks_d;
+};
 
 struct gf_ffa_program {
   int device = 0;
@@ -526,17 +658,18 @@ struct gf_ffa_program {
   std::vector<TaskDev> task_dev;
   std::vector<TrialDev> trial_dev;
   std::vector<OctaveDev> octaves;
-  std::vector<uint32_t> small_tasks, big_tasks;
+  std::vector<MetaEntry> sub_meta;
+  std::vector<uint32_t> sub_offset;
+  std::vector<FfaClass> classes;
   uint64_t nsamples = 0;
   uint64_t prep_stride = 0;
-  uint64_t max_big_elems = 0;
   uint32_t max_bins = 0, max_width = 0;
+  uint32_t pitch = 0, max_rows = 0, block_rows = 0, final_rows = 0, levels = 0;
   uint64_t halo = 0;
   uint64_t max_series = 0;
-  int big_clusters = 0;
-  int small_ctas = 0;
+  uint64_t scratch_floats = 0;
   size_t smem_bytes = 0;
-  DeviceBlob tasks_d, trials_d, octaves_d, small_d, big_d;
+  DeviceBlob tasks_d, trials_d, octaves_d, sub_meta_d, sub_offset_d;
 };
 
 namespace {
@@ -583,6 +716,47 @@ void validate_task(const gf_ffa_task& t, uint64_t n) {
   } else {
     check_arg(t.prepared_nsamples == downsampled_size_checked(n, t.downsample_factor),
               "FFA executor task prepared_nsamples must match downsampled_size");
+  }
+}
+
+uint32_t host_tree_depth(uint64_t n) {
+  uint32_t d = 0;
+  while (n > 1) { n = (n + 1) / 2; ++d; }
+  return d;
+}
+
+// Merge schedule of a subtree of n rows (ffa.cpp:127-195 recursion, by
+// depth): for level l = depth-1 .. 0 and each row r, either MERGE(head row,
+// tail row, roll) from level l+1 or CARRY(r) for rows of one-row nodes.
+void build_subtree_schedule(uint32_t n, std::vector<MetaEntry>& out) {
+  const uint32_t md = host_tree_depth(n);
+  for (int l = static_cast<int>(md) - 1; l >= 0; --l) {
+    for (uint32_t r = 0; r < n; ++r) {
+      uint32_t a = 0, sz = n, depth = 0;
+      while (depth < static_cast<uint32_t>(l) && sz > 1) {
+        const uint32_t h = sz / 2;
+        if (r - a < h) sz = h; else { a += h; sz -= h; }
+        ++depth;
+      }
+      MetaEntry m{};
+      if (depth != static_cast<uint32_t>(l) || sz < 2) {
+        m.op = kCarry;
+        m.a = static_cast<uint16_t>(r);
+      } else {
+        const uint32_t h = sz / 2, t = sz - h, s = r - a;
+        const float hsc = static_cast<float>(h - 1) / static_cast<float>(sz - 1);
+        const float tsc = static_cast<float>(t - 1) / static_cast<float>(sz - 1);
+        const float hf = hsc * static_cast<float>(s);
+        const float tf = tsc * static_cast<float>(s);
+        const uint32_t hs = static_cast<uint32_t>(hf + 0.5f);
+        const uint32_t ts = static_cast<uint32_t>(tf + 0.5f);
+        m.op = kMerge;
+        m.a = static_cast<uint16_t>(a + hs);
+        m.b = static_cast<uint16_t>(a + h + ts);
+        m.roll = static_cast<uint16_t>(s - ts);
+      }
+      out.push_back(m);
+    }
   }
 }
 
@@ -640,15 +814,43 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
     }
     check_arg(P->octaves.size() <= 32, "at most 32 distinct downsample factors");
     P->prep_stride = round_up(off, 4);
+    for (const auto& t : P->tasks) {
+      check_arg(t.bins <= kMaxBins, "FFA CUDA path supports bins <= 512");
+      check_arg(t.rows < 65536, "FFA CUDA path supports at most 65535 rows per task");
+      P->max_bins = std::max<uint32_t>(P->max_bins, static_cast<uint32_t>(t.bins));
+    }
+    for (uint64_t w : P->widths) P->max_width = std::max<uint32_t>(P->max_width, static_cast<uint32_t>(w));
+    // shared-memory geometry: two row buffers of max_rows rows, the column
+    // schedules, sized for two CTAs per SM where possible
+    P->pitch = P->max_bins | 1u;
+    P->levels = 3;
+    const size_t budget = 110 * 1024;
+    auto smem_for = [&](uint32_t rows, uint32_t K) {
+      return 2ull * rows * P->pitch * 4 + (K + 1ull) * rows * sizeof(MetaEntry) + 64;
+    };
+    uint32_t rows = 8;
+    while (smem_for(rows + 1, P->levels) <= budget) ++rows;
+    P->max_rows = rows;
+    // R + 3 (2^K - 1) rows at the bottom of a column
+    while (P->levels > 1 && static_cast<int>(rows) - 3 * ((1 << P->levels) - 1) < 8) --P->levels;
+    P->block_rows = rows - 3 * ((1u << P->levels) - 1);
+    const uint32_t cp_pitch = (P->max_bins + P->max_width + 2) | 1u;
+    P->final_rows = std::min<uint32_t>(P->block_rows, (rows * P->pitch) / cp_pitch);
+    check_arg(P->final_rows >= 1 && P->block_rows >= 1, "FFA bins too large for the shared-memory tiles");
+    P->smem_bytes = smem_for(rows, P->levels);
+    // subtree schedules for every size up to max_rows
+    P->sub_offset.assign(rows + 1, 0u);
+    for (uint32_t n = 1; n <= rows; ++n) {
+      P->sub_offset[n] = static_cast<uint32_t>(P->sub_meta.size());
+      build_subtree_schedule(n, P->sub_meta);
+    }
+    if (P->sub_meta.empty()) P->sub_meta.push_back(MetaEntry{});
+    // tasks, trials and classes
+    std::map<int, size_t> class_of;
     for (uint64_t i = 0; i < ntasks; ++i) {
       const auto& t = P->tasks[i];
-      check_arg(t.bins <= kMaxBins, "FFA CUDA path supports bins <= 512");
-      check_arg(t.rows < (1ull << 31), "FFA rows out of range");
-      uint64_t mw = 0;
-      for (uint64_t w : P->widths) {
+      for (uint64_t w : P->widths)
         check_arg(w > 0 && w < t.bins, "FFA detection width trials must satisfy 0 < width < bins");
-        mw = std::max(mw, w);
-      }
       TaskDev d{};
       d.bins = static_cast<uint32_t>(t.bins);
       d.rows = static_cast<uint32_t>(t.rows);
@@ -658,7 +860,7 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
       d.inv_stdnoise = 1.0f / task_stdnoise(t);
       d.ntrials = static_cast<uint32_t>(nwidths);
       d.trial_offset = static_cast<uint32_t>(P->trial_dev.size());
-      d.max_width = static_cast<uint32_t>(mw);
+      d.max_width = P->max_width;
       // ffa_detection.cpp:60-80 make_boxcar_trials (float arithmetic)
       const float bf = static_cast<float>(t.bins);
       for (uint64_t w : P->widths) {
@@ -666,60 +868,64 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
         const float h = std::sqrt((bf - wf) / (bf * wf));
         P->trial_dev.push_back(TrialDev{h, wf / (bf - wf) * h, static_cast<uint32_t>(w), 0u});
       }
-      // leaf depth: smallest d with ceil(rows / 2^d) <= kLeafRows
-      uint32_t dl = 0;
-      while (ceil_div(t.rows, 1ull << dl) > static_cast<uint64_t>(kLeafRows)) ++dl;
-      d.leaf_depth = dl;
+      uint32_t ds = 0;
+      while (ceil_div(t.rows, 1ull << ds) > rows) ++ds;
+      check_arg(ds <= 15, "FFA task too deep");
+      d.split_depth = ds;
       P->task_dev.push_back(d);
-      P->max_bins = std::max<uint32_t>(P->max_bins, d.bins);
-      P->max_width = std::max<uint32_t>(P->max_width, d.max_width);
-      if (dl == 0) {
-        P->small_tasks.push_back(static_cast<uint32_t>(i));
-      } else {
-        P->big_tasks.push_back(static_cast<uint32_t>(i));
-        P->max_big_elems = std::max<uint64_t>(P->max_big_elems, t.rows * t.bins);
+      int cluster = 1;
+      if (ds > 0) {
+        cluster = 0;  // medium and large tasks: scratch; cluster sized by rows
+        const uint64_t per = 512;
+        int c = 1;
+        while (c < kClusterSize && static_cast<uint64_t>(c) * per < t.rows) c *= 2;
+        cluster = c;
       }
+      // class key: 0 = on-chip (no scratch), else the cluster size
+      const int key = ds == 0 ? 0 : cluster;
+      if (!class_of.count(key)) {
+        class_of[key] = P->classes.size();
+        P->classes.emplace_back();
+        P->classes.back().cluster = ds == 0 ? 1 : cluster;
+      }
+      FfaClass& c = P->classes[class_of[key]];
+      c.tasks.push_back(static_cast<uint32_t>(i));
+      if (ds > 0) c.max_elems = std::max<uint64_t>(c.max_elems, t.rows * t.bins);
     }
-    // two kLeafRows-row transform buffers; detection batches reuse them
-    const size_t pitch = P->max_bins | 1u;
-    P->smem_bytes = 2ull * kLeafRows * pitch * sizeof(float);
-    cuda_check(cudaFuncSetAttribute(ffa_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cuda_check(cudaFuncSetAttribute(ffa_task_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(P->smem_bytes)),
-               "cudaFuncSetAttribute(ffa_small_kernel)");
-    cuda_check(cudaFuncSetAttribute(ffa_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(P->smem_bytes)),
-               "cudaFuncSetAttribute(ffa_cluster_kernel)");
-    int sms = 0, per_sm = 0;
+               "cudaFuncSetAttribute(ffa_task_kernel)");
+    cuda_check(cudaFuncSetAttribute(ffa_task_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+               "cudaFuncSetAttribute(cluster size)");
+    int sms = 0;
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_id), "device attribute");
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ffa_small_kernel, kThreads, P->smem_bytes),
-               "occupancy(ffa_small_kernel)");
-    P->small_ctas = std::max(1, sms * std::max(1, per_sm));
-    if (!P->big_tasks.empty()) {
+    for (auto& c : P->classes) {
       cudaLaunchConfig_t cfg{};
-      cfg.gridDim = dim3(kClusterSize, 1, 1);
+      cfg.gridDim = dim3(c.cluster, 1, 1);
       cfg.blockDim = dim3(kThreads, 1, 1);
       cfg.dynamicSmemBytes = P->smem_bytes;
       cudaLaunchAttribute attr{};
       attr.id = cudaLaunchAttributeClusterDimension;
-      attr.val.clusterDim.x = kClusterSize;
+      attr.val.clusterDim.x = c.cluster;
       attr.val.clusterDim.y = 1;
       attr.val.clusterDim.z = 1;
       cfg.attrs = &attr;
       cfg.numAttrs = 1;
-      int nclusters = 0;
-      cuda_check(cudaOccupancyMaxActiveClusters(&nclusters, ffa_cluster_kernel, &cfg),
-                 "cudaOccupancyMaxActiveClusters");
-      check_arg(nclusters > 0, "FFA cluster kernel cannot be resident on this device");
-      P->big_clusters = nclusters;
+      int n = 0;
+      cuda_check(cudaOccupancyMaxActiveClusters(&n, ffa_task_kernel, &cfg), "cudaOccupancyMaxActiveClusters");
+      check_arg(n > 0, "FFA kernel cannot be resident on this device");
+      c.nclusters = n;
+      if (c.max_elems) {
+        c.scratch_offset = P->scratch_floats;
+        P->scratch_floats += static_cast<uint64_t>(n) * 2 * c.max_elems;
+      }
+      c.tasks_d.upload(c.tasks.data(), c.tasks.size() * sizeof(uint32_t), device_id);
     }
-    std::vector<uint32_t> dummy{0u};
     P->tasks_d.upload(P->task_dev.data(), P->task_dev.size() * sizeof(TaskDev), device_id);
     P->trials_d.upload(P->trial_dev.data(), P->trial_dev.size() * sizeof(TrialDev), device_id);
     P->octaves_d.upload(P->octaves.data(), P->octaves.size() * sizeof(OctaveDev), device_id);
-    const auto& sm_list = P->small_tasks.empty() ? dummy : P->small_tasks;
-    const auto& bg_list = P->big_tasks.empty() ? dummy : P->big_tasks;
-    P->small_d.upload(sm_list.data(), sm_list.size() * sizeof(uint32_t), device_id);
-    P->big_d.upload(bg_list.data(), bg_list.size() * sizeof(uint32_t), device_id);
+    P->sub_meta_d.upload(P->sub_meta.data(), P->sub_meta.size() * sizeof(MetaEntry), device_id);
+    P->sub_offset_d.upload(P->sub_offset.data(), P->sub_offset.size() * sizeof(uint32_t), device_id);
     *out = P.release();
   });
 }
@@ -735,11 +941,14 @@ extern "C" int gf_ffa_program_info(const gf_ffa_program* P, gf_ffa_info* info) {
     info->ntasks = P->tasks.size();
     info->noctaves = P->octaves.size();
     info->prepared_floats = P->prep_stride;
-    info->scratch_bytes = static_cast<uint64_t>(std::max(1, P->big_clusters)) * 2 * std::max<uint64_t>(1, P->max_big_elems) * 4;
+    info->scratch_bytes = std::max<uint64_t>(16, P->scratch_floats * 4);
     uint64_t mx = 0;
     for (const auto& t : P->tasks) mx = std::max<uint64_t>(mx, t.rows * t.bins);
     info->max_task_elements = mx;
-    info->metadata_bytes = P->tasks_d.bytes + P->trials_d.bytes + P->octaves_d.bytes + P->small_d.bytes + P->big_d.bytes;
+    info->metadata_bytes = P->tasks_d.bytes + P->trials_d.bytes + P->octaves_d.bytes + P->sub_meta_d.bytes +
+                           P->sub_offset_d.bytes;
+    for (const auto& c : P->classes) info->metadata_bytes += c.tasks_d.bytes;
+    info->nclasses = P->classes.size();
   });
 }
 
@@ -771,6 +980,7 @@ extern "C" int gf_ffa_search(gf_ffa_program* P, const float* dev_prepared, uint6
     check_arg(std::isfinite(snr_threshold), "FFA search S/N threshold must be finite");
     check_arg(nseries > 0 && nseries <= P->max_series, "nseries must be in (0, max_series]");
     check_arg(capacity == 0 || dev_peaks != nullptr, "peak buffer must not be null");
+    check_arg(P->scratch_floats == 0 || dev_scratch != nullptr, "FFA search needs scratch");
     DeviceGuard dg(P->device);
     auto s = as_stream(stream);
     cuda_check(cudaMemsetAsync(dev_counters, 0, 2 * sizeof(uint64_t), s), "cudaMemsetAsync(counters)");
@@ -779,32 +989,41 @@ extern "C" int gf_ffa_search(gf_ffa_program* P, const float* dev_prepared, uint6
     sp.prep_stride = P->prep_stride;
     sp.tasks = P->tasks_d.as<TaskDev>();
     sp.trials = P->trials_d.as<TrialDev>();
+    sp.sub_meta = P->sub_meta_d.as<MetaEntry>();
+    sp.sub_offset = P->sub_offset_d.as<uint32_t>();
     sp.nseries = static_cast<uint32_t>(nseries);
     sp.threshold = snr_threshold;
     sp.peaks = dev_peaks;
     sp.capacity = capacity;
     sp.counters = reinterpret_cast<unsigned long long*>(dev_counters);
-    sp.max_bins = P->max_bins;
-    sp.smem_pitch = P->max_bins | 1u;
-    if (!P->small_tasks.empty()) {
-      sp.item_tasks = P->small_d.as<uint32_t>();
-      sp.nitem_tasks = static_cast<uint32_t>(P->small_tasks.size());
-      const uint64_t items = nseries * P->small_tasks.size();
-      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(items, static_cast<uint64_t>(P->small_ctas)));
-      ffa_small_kernel<<<grid, kThreads, P->smem_bytes, s>>>(sp);
-      cuda_check(cudaGetLastError(), "ffa_small_kernel launch");
-    }
-    if (!P->big_tasks.empty()) {
-      check_arg(dev_scratch != nullptr, "FFA search needs scratch for large tasks");
-      sp.item_tasks = P->big_d.as<uint32_t>();
-      sp.nitem_tasks = static_cast<uint32_t>(P->big_tasks.size());
-      sp.scratch = static_cast<float*>(dev_scratch);
-      sp.scratch_elems = P->max_big_elems;
-      const uint64_t items = nseries * P->big_tasks.size();
-      const unsigned nclusters =
-          static_cast<unsigned>(std::min<uint64_t>(items, static_cast<uint64_t>(P->big_clusters)));
-      ffa_cluster_kernel<<<nclusters * kClusterSize, kThreads, P->smem_bytes, s>>>(sp);
-      cuda_check(cudaGetLastError(), "ffa_cluster_kernel launch");
+    sp.pitch = P->pitch;
+    sp.max_rows = P->max_rows;
+    sp.block_rows = P->block_rows;
+    sp.final_rows = P->final_rows;
+    sp.levels = P->levels;
+    sp.error = reinterpret_cast<uint32_t*>(dev_counters + 1);
+    // largest tasks first so the long clusters start early
+    for (auto it = P->classes.rbegin(); it != P->classes.rend(); ++it) {
+      const FfaClass& c = *it;
+      sp.item_tasks = c.tasks_d.as<uint32_t>();
+      sp.nitem_tasks = static_cast<uint32_t>(c.tasks.size());
+      sp.scratch = c.max_elems ? static_cast<float*>(dev_scratch) + c.scratch_offset : nullptr;
+      sp.scratch_elems = c.max_elems;
+      const uint64_t items = nseries * c.tasks.size();
+      const unsigned nclusters = static_cast<unsigned>(std::min<uint64_t>(items, static_cast<uint64_t>(c.nclusters)));
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(nclusters * c.cluster, 1, 1);
+      cfg.blockDim = dim3(kThreads, 1, 1);
+      cfg.dynamicSmemBytes = P->smem_bytes;
+      cfg.stream = s;
+      cudaLaunchAttribute attr{};
+      attr.id = cudaLaunchAttributeClusterDimension;
+      attr.val.clusterDim.x = c.cluster;
+      attr.val.clusterDim.y = 1;
+      attr.val.clusterDim.z = 1;
+      cfg.attrs = &attr;
+      cfg.numAttrs = 1;
+      cuda_check(cudaLaunchKernelEx(&cfg, ffa_task_kernel, sp), "ffa_task_kernel launch");
     }
   });
 }

@@ -118,7 +118,7 @@ class DmSearch:
         parts = []
         launches = 0
         dd_kernels = 1 if self.dedisp.algorithm == "brute" else 2
-        ffa_kernels = int(self.ffa.has_small) + int(self.ffa.has_big)
+        ffa_kernels = self.ffa.kernel_launches
         for b0 in range(0, self.ndm, self.dm_batch):
             cnt = min(self.dm_batch, self.ndm - b0)
             with _StageTimer(timers, "dedisperse"):

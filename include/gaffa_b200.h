@@ -38,6 +38,7 @@ extern "C" {
 #define GF_STATUS_NONFINITE 1u
 #define GF_STATUS_CONSTANT 2u
 #define GF_STATUS_PEAK_OVERFLOW 4u
+#define GF_STATUS_SCHEDULE 8u /* an FFA block schedule exceeded its tile (internal error) */
 
 const char* gf_last_error(void);
 const char* gf_status_string(int status);
@@ -220,6 +221,7 @@ typedef struct {
   uint64_t scratch_bytes;       /* per gf_ffa_search call */
   uint64_t max_task_elements;   /* rows * bins of the largest task */
   uint64_t metadata_bytes;
+  uint64_t nclasses;            /* kernel launches per gf_ffa_search */
 } gf_ffa_info;
 
 /* Compact device peak record (24 bytes); FfaCudaPeak of
