@@ -140,6 +140,8 @@ _SIGNATURES = [
     ("gf_fold_workspace_bytes", u64, [u64, u64]),
     ("gf_fold_time_series", C.c_int, [vp, i32, u64, dbl, dbl, u64, u64, vp, vp, vp, vp]),
     ("gf_synth_generate", C.c_int, [C.POINTER(SynthDesc), u64, u64, vp, vp]),
+    ("gf_fold_noalloc_max_bytes", u64, []),
+    ("gf_fold_time_series_noalloc", C.c_int, [vp, i32, u64, dbl, dbl, u64, u64, vp, vp, vp, vp]),
 ]
 
 ENTRY_POINTS = [name for name, _, _ in _SIGNATURES]

@@ -16,6 +16,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 
 namespace gf {
 namespace {
@@ -130,6 +132,95 @@ extern "C" int gf_fold_time_series(const void* dev_input, int32_t input_is_u32, 
                                       static_cast<int>(smem)), "cudaFuncSetAttribute(fold)");
       fold_partial_kernel<false><<<static_cast<unsigned>(blocks), kThreads, smem, s>>>(
           dev_input, n, step, start_sample, nbin, partial, status);
+    }
+    fold_reduce_kernel<<<static_cast<unsigned>(ceil_div(nbin, kThreads)), kThreads, 0, s>>>(
+        partial, static_cast<int>(blocks), nbin, dev_profile, dev_exposure);
+    cuda_check(cudaGetLastError(), "fold launch");
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Fold without any device allocation.
+//
+// Some callers cannot allocate device memory when they fold: a process whose
+// device memory has all been handed to another allocator's pool, or a
+// latency-critical loop where cudaMalloc's implicit device synchronisation is
+// not acceptable.  gf_fold_time_series_noalloc serves them with a fixed
+// scratch area compiled into this library: a file-scope device array that
+// every GPU which loads the library holds until the process exits.  Its size
+// caps the work: fold_blocks(n) * 2 * nbin doubles must fit in
+// kNoAllocScratchBytes (4 MiB: e.g. nbin = 64 up to ~67 million samples).
+// All calls share the array and it keeps the last call's contents; the
+// partial sums are fully rewritten by every call, so nothing needs clearing,
+// but calls that overlap on the GPU (different streams, or different host
+// threads) race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr uint64_t kNoAllocScratchBytes = 4ull << 20;
+static __device__ __align__(256) unsigned char g_fold_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_fold_scratch_mutex;
+void* g_fold_scratch_address[kMaxDevices] = {};
+
+// Device address of g_fold_scratch on the current device, resolved once per
+// device.  In host code the array's name is only a host-side stand-in, so
+// the kernels must receive this address, never &g_fold_scratch.
+void* fold_scratch_address() {
+  int device = -1;
+  cuda_check(cudaGetDevice(&device), "cudaGetDevice");
+  check_arg(device >= 0 && device < kMaxDevices, "device ordinal out of range for the fixed fold scratch");
+  std::lock_guard<std::mutex> lock(g_fold_scratch_mutex);
+  if (g_fold_scratch_address[device] == nullptr) {
+    void* ptr = nullptr;
+    cuda_check(cudaGetSymbolAddress(&ptr, g_fold_scratch), "cudaGetSymbolAddress(fold scratch)");
+    g_fold_scratch_address[device] = ptr;
+  }
+  return g_fold_scratch_address[device];
+}
+
+}  // namespace
+
+extern "C" uint64_t gf_fold_noalloc_max_bytes(void) { return kNoAllocScratchBytes; }
+
+extern "C" int gf_fold_time_series_noalloc(const void* dev_input, int32_t input_is_u32, uint64_t n, double period,
+                                           double tsamp, uint64_t nbin, uint64_t start_sample, float* dev_profile,
+                                           double* dev_exposure, uint32_t* dev_status, void* stream) {
+  return guarded([&] {
+    check_arg(n > 0, "fold input must not be empty");
+    check_arg(nbin > 0, "fold nbin must be positive");
+    const uint64_t need = fold_blocks(n) * 2 * nbin * sizeof(double);
+    if (need > kNoAllocScratchBytes) {
+      raise(GF_EINVAL, "fold without allocation: " + std::to_string(n) + " samples x " + std::to_string(nbin) +
+                           " bins need " + std::to_string(need) + " bytes of scratch, above the fixed " +
+                           std::to_string(kNoAllocScratchBytes) + " bytes; use gf_fold_time_series");
+    }
+    // folding.cpp:44-73 validation, as gf_fold_time_series
+    check_arg(std::isfinite(period) && period > 0.0, "fold period must be finite and positive");
+    check_arg(std::isfinite(tsamp) && tsamp > 0.0, "fold tsamp must be finite and positive");
+    check_arg(nbin <= kMaxBins, "CUDA fold supports nbin <= 8192");
+    check_arg(dev_input && dev_profile && dev_exposure && dev_status, "null argument");
+    const double step = tsamp / period * static_cast<double>(nbin);
+    const double hi = static_cast<double>(start_sample + n - 1) * step + step;
+    check_arg(std::isfinite(hi) && std::ceil(hi) < 9.2e18, "fold phase bin index exceeds int64 range");
+    auto s = as_stream(stream);
+    const uint64_t blocks = fold_blocks(n);
+    double* partial = static_cast<double*>(fold_scratch_address());
+    // the status word must start at zero; the partial sums are overwritten
+    cuda_check(cudaMemsetAsync(dev_status, 0, 4, s), "cudaMemsetAsync(fold status)");
+    const size_t smem = 2 * nbin * sizeof(double);
+    if (input_is_u32) {
+      cuda_check(cudaFuncSetAttribute(fold_partial_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(smem)), "cudaFuncSetAttribute(fold)");
+      fold_partial_kernel<true><<<static_cast<unsigned>(blocks), kThreads, smem, s>>>(
+          dev_input, n, step, start_sample, nbin, partial, dev_status);
+    } else {
+      cuda_check(cudaFuncSetAttribute(fold_partial_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(smem)), "cudaFuncSetAttribute(fold)");
+      fold_partial_kernel<false><<<static_cast<unsigned>(blocks), kThreads, smem, s>>>(
+          dev_input, n, step, start_sample, nbin, partial, dev_status);
     }
     fold_reduce_kernel<<<static_cast<unsigned>(ceil_div(nbin, kThreads)), kThreads, 0, s>>>(
         partial, static_cast<int>(blocks), nbin, dev_profile, dev_exposure);

@@ -363,6 +363,27 @@ int gf_fold_time_series(const void* dev_input, int32_t input_is_u32, uint64_t n,
                         uint64_t start_sample, float* dev_profile,
                         double* dev_exposure, void* dev_workspace, void* stream);
 
+/* Fold without allocating device memory.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc at fold time -- a process whose
+ * device memory is all owned by another allocator's pool, or a
+ * latency-critical loop that cannot afford cudaMalloc's implicit device
+ * synchronisation.  Same arithmetic as gf_fold_time_series, but the per-block
+ * partial sums live in a fixed scratch array compiled into the library (held
+ * by every GPU that loads it until exit), so the work is capped:
+ * ceil(n / 16384) * 2 * nbin doubles must fit in gf_fold_noalloc_max_bytes()
+ * bytes (4 MiB; e.g. nbin = 64 allows about 67 million samples); larger
+ * requests fail with GF_EINVAL.  dev_status (caller-owned, uint32) receives
+ * GF_STATUS_NONFINITE for non-finite float input.  The first call on a
+ * device resolves the array's device address for that device (call it once
+ * before any stream capture).  All calls share the array: calls that
+ * overlap on the GPU race on it and must be serialised by the caller. */
+uint64_t gf_fold_noalloc_max_bytes(void);
+int gf_fold_time_series_noalloc(const void* dev_input, int32_t input_is_u32,
+                                uint64_t n, double period, double tsamp,
+                                uint64_t nbin, uint64_t start_sample,
+                                float* dev_profile, double* dev_exposure,
+                                uint32_t* dev_status, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Synthetic observations (no reference counterpart)                         */
 /* ------------------------------------------------------------------------ */
