@@ -90,6 +90,17 @@ struct DeviceBlob {
     o.ptr = nullptr;
     o.bytes = 0;
   }
+  DeviceBlob& operator=(DeviceBlob&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      bytes = o.bytes;
+      device = o.device;
+      o.ptr = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
   ~DeviceBlob() { release(); }
   void release() {
     if (ptr) {

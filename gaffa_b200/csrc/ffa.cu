@@ -17,11 +17,13 @@
 // is the input row itself.  A task whose rows fit a CTA's shared memory runs in
 // one CTA (all levels on chip, root rows fed straight into detection).  Larger
 // tasks run on a thread-block cluster: each CTA transforms subtrees of at most
-// kLeafRows rows on chip and writes them to the cluster's global scratch,
-// then the cluster steps up the tree one depth per cluster barrier (rows
-// split across its CTAs, scratch kept hot in L2), and the root level is fused
-// with detection.  No CTA ever waits on another except through the hardware
-// cluster barrier.
+// max_rows rows on chip and writes them to the cluster's global scratch; then
+// column passes of up to three levels each climb to the root.  A column block
+// computes a run of rows of one node from the rows three levels down that it
+// depends on (the schedules are built on the host, once per program); blocks
+// of a pass are split across the cluster's CTAs, and a hardware cluster
+// barrier separates passes.  The root pass is fused with detection.  Kernels
+// are instantiated per NB = ceil(bins / 32) so every row loop is unrolled.
 #include "common.cuh"
 
 #include <cooperative_groups.h>
@@ -39,7 +41,6 @@ namespace gf {
 namespace {
 
 constexpr int kThreads = 512;
-constexpr int kLeafRows = 64;       // rows transformed on chip per subtree
 constexpr int kMaxBins = 512;
 constexpr int kMaxWidths = 64;
 constexpr int kClusterSize = 8;
@@ -53,6 +54,8 @@ struct TaskDev {
   uint32_t trial_offset;
   uint32_t split_depth;   // depth of the on-chip subtrees (0: whole task in one CTA)
   uint32_t max_width;
+  uint32_t pass_begin;    // column passes (split_depth > 0)
+  uint32_t npasses;
   uint32_t reserved;
 };
 
@@ -155,13 +158,15 @@ __global__ void __launch_bounds__(kThreads) prepare_kernel(const float* __restri
 // A level of the tree is a list of rows, each produced by one MetaEntry:
 //   MERGE  out = prev[a] + roll_left(prev[b], roll mod bins)   (ffa.cpp:110-171)
 //   CARRY  out = prev[a]              (a one-row node carried up unchanged)
-//   LOAD   out = global row a         (input rows or rows of a lower pass)
 // Rows of a level live in one of two shared-memory buffers (pitch = bins|1);
-// levels alternate buffers, so each level costs one __syncthreads.
+// levels alternate buffers, so each level costs one __syncthreads.  Every
+// loop over the bins of a row is unrolled for NB = ceil(bins / 32) (the
+// kernels are instantiated per NB), so a merged element costs two shared
+// loads, one add and one shared store.
 
-enum : uint16_t { kMerge = 0, kCarry = 1, kLoad = 2 };
+enum : uint16_t { kMerge = 0, kCarry = 1 };
 
-struct MetaEntry {
+struct __align__(8) MetaEntry {
   uint16_t op, a, b, roll;
 };
 
@@ -186,7 +191,7 @@ __device__ __forceinline__ Node node_of(uint32_t r, uint32_t n, uint32_t depth) 
 }
 
 // Node `index` (bits read MSB first, 0 = head) at depth `depth`.
-__device__ __forceinline__ Node node_at(uint32_t index, uint32_t n, uint32_t depth) {
+__host__ __device__ __forceinline__ Node node_at(uint32_t index, uint32_t n, uint32_t depth) {
   Node nd{0u, n, depth};
   for (uint32_t b = depth; b-- > 0;) {
     const uint32_t h = nd.n >> 1;
@@ -208,53 +213,114 @@ __device__ __forceinline__ uint32_t scaled_shift(float scale, uint32_t s) {
   return static_cast<uint32_t>(__fadd_rn(__fmul_rn(scale, static_cast<float>(s)), 0.5f));
 }
 
-template <bool GlobalCg>
-__device__ __forceinline__ void eval_level(const MetaEntry* __restrict__ meta, uint32_t nrows,
-                                           const float* __restrict__ prev, float* __restrict__ out,
-                                           uint32_t pitch, const float* __restrict__ gsrc, uint32_t bins) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t q = warp; q < nrows; q += kThreads / 32) {
+__host__ __device__ __forceinline__ uint32_t tree_depth(uint32_t n) {
+  uint32_t d = 0;
+  while (n > 1) { n = (n + 1) >> 1; ++d; }
+  return d;
+}
+
+// A column block of a pass (built on the host): rows [s0, s1) of one node X
+// at depth dx, evaluated from the rows of depth dx + levels that they depend
+// on.  Level k (0 = X) holds count[k] rows; the bottom level is loaded from
+// the pass's source scratch as up to 8 runs of consecutive task rows.
+struct ColBlock {
+  uint32_t meta;          // first merge entry: levels-1, ..., 0 back to back
+  uint32_t out_row;       // final pass: shift of the first root row; else task row of the first output row
+  uint16_t count[4];      // rows at relative level 0 .. levels
+  uint16_t run_off[8];    // bottom level: buffer row where each run starts
+  uint16_t run_row[8];    // bottom level: task row where each run starts
+  uint8_t levels, final_pass, nruns, reserved;
+  uint32_t pad[3];
+};
+static_assert(sizeof(ColBlock) == 64, "ColBlock is 16 words");
+
+struct PassDev {
+  uint32_t block_begin, nblocks;
+};
+
+constexpr int kWarps = kThreads / 32;
+
+// Dynamic shared memory of the search kernel: two ColBlock headers, the
+// staged schedule, then two row buffers.  The row buffers start at least
+// max_bins floats in, so a row pointer minus bins stays inside the block's
+// allocation.
+extern __shared__ __align__(16) float g_smem[];
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// One level: out row q (q < nrows) from `prev` by meta[q].  A warp per row,
+// lane j handles bins j, j+32, ...; only the last iteration can be partial.
+// The tail row is read at (j + roll) mod bins: a lane reads from t1 = tail +
+// roll + j until its index passes bins, then from t2 = t1 - bins.
+template <int NB>
+__device__ __forceinline__ void merge_level(const MetaEntry* meta, uint32_t nrows, const float* prev, float* out,
+                                            uint32_t pitch, uint32_t bins) {
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool last_ok = lane + 32u * (NB - 1) < bins;
+  for (uint32_t q = warp; q < nrows; q += kWarps) {
     const MetaEntry m = meta[q];
-    float* o = out + q * pitch;
+    float* o = out + q * pitch + lane;
+    const float* h = prev + m.a * pitch + lane;
     if (m.op == kMerge) {
-      const float* h = prev + m.a * pitch;
-      const float* t = prev + m.b * pitch;
-      const uint32_t r = m.roll < bins ? m.roll : m.roll % bins;
-      for (uint32_t j = lane; j < bins; j += 32) {
-        uint32_t k = j + r;
-        if (k >= bins) k -= bins;
-        o[j] = __fadd_rn(h[j], t[k]);
+      uint32_t r = m.roll;
+      if (r >= bins) r %= bins;
+      const uint32_t base = lane + r;
+      const int iw = (static_cast<int>(bins) - static_cast<int>(base) + 31) >> 5;  // unwrapped iterations
+      const float* t1 = prev + m.b * pitch + base;
+      const float* t2 = t1 - bins;
+#pragma unroll
+      for (int i = 0; i < NB; ++i) {
+        if (i < NB - 1 || last_ok) {
+          const float* t = i < iw ? t1 : t2;
+          o[32 * i] = __fadd_rn(h[32 * i], t[32 * i]);
+        }
       }
-    } else if (m.op == kCarry) {
-      const float* h = prev + m.a * pitch;
-      for (uint32_t j = lane; j < bins; j += 32) o[j] = h[j];
     } else {
-      const float* g = gsrc + static_cast<uint64_t>(m.a) * bins;
-      for (uint32_t j = lane; j < bins; j += 32) o[j] = GlobalCg ? __ldcg(g + j) : __ldg(g + j);
+#pragma unroll
+      for (int i = 0; i < NB; ++i)
+        if (i < NB - 1 || last_ok) o[32 * i] = h[32 * i];
     }
   }
 }
 
-// rows [0, n) of `src` (global, pitch bins, row a0 first) into smem
-template <bool GlobalCg>
-__device__ __forceinline__ void load_rows(const float* src, uint32_t n, uint32_t bins, float* out, uint32_t pitch) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t q = warp; q < n; q += kThreads / 32)
-    for (uint32_t j = lane; j < bins; j += 32)
-      out[q * pitch + j] = GlobalCg ? __ldcg(src + static_cast<uint64_t>(q) * bins + j)
-                                    : __ldg(src + static_cast<uint64_t>(q) * bins + j);
+// rows [0, n) of read-only global `src` (row length bins) into smem, async
+template <int NB>
+__device__ __forceinline__ void load_rows_async(const float* src, uint32_t n, uint32_t bins, float* out,
+                                                uint32_t pitch) {
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool last_ok = lane + 32u * (NB - 1) < bins;
+  for (uint32_t q = warp; q < n; q += kWarps) {
+    const float* g = src + static_cast<uint64_t>(q) * bins + lane;
+    float* o = out + q * pitch + lane;
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+      if (i < NB - 1 || last_ok) cp_async4(o + 32 * i, g + 32 * i);
+  }
 }
 
+template <int NB>
 __device__ __forceinline__ void store_rows(const float* in, uint32_t pitch, uint32_t n, uint32_t bins, float* dst) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t q = warp; q < n; q += kThreads / 32)
-    for (uint32_t j = lane; j < bins; j += 32) __stcg(dst + static_cast<uint64_t>(q) * bins + j, in[q * pitch + j]);
-}
-
-__device__ __forceinline__ uint32_t tree_depth(uint32_t n) {
-  uint32_t d = 0;
-  while (n > 1) { n = (n + 1) >> 1; ++d; }
-  return d;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool last_ok = lane + 32u * (NB - 1) < bins;
+  for (uint32_t q = warp; q < n; q += kWarps) {
+    float* g = dst + static_cast<uint64_t>(q) * bins + lane;
+    const float* s = in + q * pitch + lane;
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+      if (i < NB - 1 || last_ok) __stcg(g + 32 * i, s[32 * i]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -271,19 +337,33 @@ struct DetectArgs {
   unsigned long long* counters;
 };
 
+// order-preserving map of finite floats to unsigned keys (for redux.sync)
+__device__ __forceinline__ uint32_t float_key(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
 // rows[i] (pitch `pitch`) hold root rows shift0 + i, i < count.  Prefix sums
-// are sequential per row (one thread per row, ffa_detection.cpp:126-139);
-// each warp then scans one row for every width (first phase of the maximum,
-// :141-170) and appends peaks with S/N >= threshold.
+// are sequential per row (one thread per row, ffa_detection.cpp:126-139).
+// Then a warp per row: lane j holds c[j + 32i] and, for every width, takes
+// the maximum of c[ph + w] - c[ph] over its phases; redux.sync gives the
+// row maximum, from which S/N follows (:141-170).  Only when S/N passes the
+// threshold is the first phase attaining the maximum looked up (the
+// reference's strict '>' scan keeps the first maximum), and a peak appended.
+template <int NB>
 __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, uint32_t shift0, float* cp,
                             uint32_t cp_pitch, const DetectArgs& a) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t bins = a.bins;
   if (threadIdx.x < count) {
     const float* prof = rows + threadIdx.x * pitch;
     float* c = cp + threadIdx.x * cp_pitch;
     float acc = 0.0f;
     c[0] = 0.0f;
+#pragma unroll 8
     for (uint32_t i = 0; i < bins; ++i) {
       acc = __fadd_rn(acc, prof[i]);
       c[i + 1] = acc;
@@ -294,35 +374,38 @@ __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, u
     }
   }
   __syncthreads();
-  for (uint32_t r = warp; r < count; r += kThreads / 32) {
-    const float* c = cp + r * cp_pitch;
-    const float psum = c[bins];
+  const bool last_ok = lane + 32u * (NB - 1) < bins;
+  for (uint32_t r = warp; r < count; r += kWarps) {
+    const float* c = cp + r * cp_pitch + lane;
+    float base[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) base[i] = (i < NB - 1 || last_ok) ? c[32 * i] : 0.0f;
+    const float psum = cp[r * cp_pitch + bins];
     for (uint32_t k = 0; k < a.ntrials; ++k) {
       const TrialDev tr = a.trials[k];
+      const float* cw = c + tr.width;
       float best = -INFINITY;
-      uint32_t best_ph = 0xffffffffu;
-      for (uint32_t ph = lane; ph < bins; ph += 32) {
-        const float v = __fsub_rn(c[ph + tr.width], c[ph]);
-        if (v > best) { best = v; best_ph = ph; }
-      }
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const float ov = __shfl_xor_sync(0xffffffffu, best, off);
-        const uint32_t op = __shfl_xor_sync(0xffffffffu, best_ph, off);
-        if (ov > best || (ov == best && op < best_ph)) { best = ov; best_ph = op; }
-      }
-      if (lane == 0) {
-        const float snr = __fmul_rn(
-            __fsub_rn(__fmul_rn(__fadd_rn(tr.height, tr.baseline), best), __fmul_rn(tr.baseline, psum)),
-            a.inv_stdnoise);
-        if (snr >= a.threshold) {
+      for (int i = 0; i < NB; ++i)
+        if (i < NB - 1 || last_ok) best = fmaxf(best, __fsub_rn(cw[32 * i], base[i]));
+      const float maxv = key_float(__reduce_max_sync(0xffffffffu, float_key(best)));
+      const float snr = __fmul_rn(
+          __fsub_rn(__fmul_rn(__fadd_rn(tr.height, tr.baseline), maxv), __fmul_rn(tr.baseline, psum)),
+          a.inv_stdnoise);
+      if (snr >= a.threshold) {  // warp-uniform: maxv is the same on every lane
+        uint32_t first = 0xffffffffu;
+#pragma unroll
+        for (int i = NB - 1; i >= 0; --i)
+          if ((i < NB - 1 || last_ok) && __fsub_rn(cw[32 * i], base[i]) == maxv) first = lane + 32u * i;
+        const uint32_t ph = __reduce_min_sync(0xffffffffu, first);
+        if (lane == 0) {
           const unsigned long long slot = atomicAdd(a.counters, 1ull);
           if (slot < a.capacity) {
             gf_peak_record rec;
             rec.series = a.series;
             rec.task = a.task;
             rec.shift = shift0 + r;
-            rec.phase = static_cast<uint16_t>(best_ph);
+            rec.phase = static_cast<uint16_t>(ph);
             rec.width_index = static_cast<uint16_t>(k);
             rec.snr = snr;
             rec.reserved = 0u;
@@ -344,6 +427,9 @@ struct SearchParams {
   const TrialDev* trials;
   const MetaEntry* sub_meta;    // subtree schedules by size
   const uint32_t* sub_offset;   // [max_rows + 1]
+  const MetaEntry* col_meta;    // column-block merge entries
+  const ColBlock* blocks;       // column blocks, pass by pass
+  const PassDev* passes;
   const uint32_t* item_tasks;   // task indices of this launch's class
   uint32_t nitem_tasks;
   uint32_t nseries;
@@ -355,10 +441,7 @@ struct SearchParams {
   uint64_t scratch_elems;
   uint32_t pitch;               // shared-memory row pitch (max bins | 1)
   uint32_t max_rows;            // rows per shared-memory buffer
-  uint32_t block_rows;          // R: output rows per column block
-  uint32_t final_rows;          // R for the root pass (room for prefix sums)
-  uint32_t levels;              // K: levels per column pass
-  uint32_t* error;              // set when a schedule would overflow a buffer
+  uint32_t front;               // floats before the first row buffer
 };
 
 __device__ __forceinline__ DetectArgs make_detect(const SearchParams& p, const TaskDev& t, uint32_t series,
@@ -378,159 +461,93 @@ __device__ __forceinline__ DetectArgs make_detect(const SearchParams& p, const T
   return da;
 }
 
-// Evaluates a whole subtree of n <= max_rows rows starting at input row
-// `a` (pointer `src` = row a), from its input rows up to relative level
-// `stop` (0: the subtree root).  Returns the buffer holding level `stop`.
+// Evaluates a whole subtree of n <= max_rows rows (pointer `src` = its first
+// input row) from its input rows up to relative level `stop` (0: the
+// subtree root).  The subtree's schedule (depth x n entries, level depth-1
+// first) is left in cmeta.  Returns the buffer holding level `stop`.
+template <int NB>
 __device__ float* eval_subtree(const SearchParams& p, const float* src, uint32_t n, uint32_t bins, uint32_t stop,
-                               float* buf0, float* buf1) {
+                               float* buf0, float* buf1, MetaEntry* cmeta) {
   const uint32_t pitch = p.pitch;
   const uint32_t md = tree_depth(n);
-  float* bufs[2] = {buf0, buf1};
-  load_rows<false>(src, n, bins, bufs[md & 1], pitch);
-  __syncthreads();
   const MetaEntry* table = p.sub_meta + p.sub_offset[n];
+  for (uint32_t e = threadIdx.x; e < md * n; e += kThreads) cp_async8(cmeta + e, table + e);
+  load_rows_async<NB>(src, n, bins, (md & 1) ? buf1 : buf0, pitch);
+  cp_async_wait_all();
+  __syncthreads();
   for (int l = static_cast<int>(md) - 1; l >= static_cast<int>(stop); --l) {
-    eval_level<false>(table + (md - 1 - l) * n, n, bufs[(l + 1) & 1], bufs[l & 1], pitch, nullptr, bins);
+    merge_level<NB>(cmeta + (md - 1 - l) * n, n, ((l + 1) & 1) ? buf1 : buf0, (l & 1) ? buf1 : buf0, pitch, bins);
     __syncthreads();
   }
-  return bufs[stop & 1];
+  return (stop & 1) ? buf1 : buf0;
 }
 
-// Column block: rows [s0, s1) of node X (task rows, depth dx) computed from
-// the rows of depth dx + K held in global `src` (task row coordinates).
-// Warp 0 builds the per-level row schedules top-down (only the rows the
-// block needs, ffa.cpp index arithmetic); all warps then evaluate bottom-up.
-// The result (s1 - s0 rows) is in buf0.
-__device__ void eval_column(const SearchParams& p, Node X, uint32_t s0, uint32_t s1, uint32_t K, const float* src,
-                            uint32_t bins, float* buf0, float* buf1, MetaEntry* cmeta, uint32_t* counts) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t max_rows = p.max_rows;
-  if (warp == 0) {
-    // per level: up to 2^k nodes (K <= 3 -> <= 8), one per lane
-    uint32_t na = 0, nn = 0, nu0 = 0, nu1 = 0, noff = 0;  // this lane's node at the current level
-    uint32_t count = 1;
-    if (lane == 0) { na = X.a; nn = X.n; nu0 = s0; nu1 = s1; noff = 0; }
-    uint32_t rows = s1 - s0;
-    bool overflow = rows > max_rows;
-    for (uint32_t k = 0; k < K; ++k) {
-      // children of this lane's node
-      uint32_t ha = 0, hn = 0, hu0 = 0, hu1 = 0, ta = 0, tn = 0, tu0 = 0, tu1 = 0;
-      float hsc = 0.0f, tsc = 0.0f;
-      if (lane < count) {
-        const uint32_t h = nn >> 1, t = nn - h;
-        hsc = shift_scale(h, nn);
-        tsc = shift_scale(t, nn);
-        ha = na; hn = h; hu0 = scaled_shift(hsc, nu0); hu1 = scaled_shift(hsc, nu1 - 1) + 1;
-        ta = na + h; tn = t; tu0 = scaled_shift(tsc, nu0); tu1 = scaled_shift(tsc, nu1 - 1) + 1;
-      }
-      // offsets of the children rows at level k+1 (exclusive scan, head then tail)
-      const uint32_t len = (hu1 - hu0) + (tu1 - tu0);
-      uint32_t incl = len;
+// Column block `hb`: stages its merge entries, loads its bottom rows from
+// `src` (scratch written by other CTAs of the cluster: L2 loads), evaluates
+// its levels.  The output rows (hb.count[0]) end in buf0.
+template <int NB>
+__device__ void eval_block(const SearchParams& p, const ColBlock& hb, const float* src, uint32_t bins, float* buf0,
+                           float* buf1, MetaEntry* cmeta) {
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t pitch = p.pitch;
+  const uint32_t K = hb.levels;
+  uint32_t nmeta = 0;
+  for (uint32_t k = 0; k < K; ++k) nmeta += hb.count[k];
+  const MetaEntry* gm = p.col_meta + hb.meta;  // 16-byte aligned, padded to an even count
+  for (uint32_t e = 2 * threadIdx.x; e < nmeta; e += 2 * kThreads) cp_async16(cmeta + e, gm + e);
+  float* bottom = (K & 1) ? buf1 : buf0;
+  const uint32_t nb = hb.count[K];
+  const uint32_t nruns = hb.nruns;
+  const bool last_ok = lane + 32u * (NB - 1) < bins;
+  for (uint32_t q = warp; q < nb; q += kWarps) {
+    uint32_t j = 0;
+    while (j + 1 < nruns && hb.run_off[j + 1] <= q) ++j;
+    const float* g = src + static_cast<uint64_t>(hb.run_row[j] + (q - hb.run_off[j])) * bins + lane;
+    float v[NB];
 #pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= off) incl += v;
-      }
-      const uint32_t hoff = incl - len, toff = hoff + (hu1 - hu0);
-      const uint32_t next_rows = __shfl_sync(0xffffffffu, incl, 31);
-      overflow |= next_rows > max_rows;
-      if (lane == 0) counts[k + 1] = next_rows;
-      // schedule of level k: rows of each node, lanes over rows
-      MetaEntry* mk = cmeta + k * max_rows;
-      for (uint32_t i = 0; i < count; ++i) {
-        const uint32_t bu0 = __shfl_sync(0xffffffffu, nu0, i), bu1 = __shfl_sync(0xffffffffu, nu1, i);
-        const uint32_t boff = __shfl_sync(0xffffffffu, noff, i);
-        const float bh = __shfl_sync(0xffffffffu, hsc, i), bt = __shfl_sync(0xffffffffu, tsc, i);
-        const uint32_t bho = __shfl_sync(0xffffffffu, hoff, i), bto = __shfl_sync(0xffffffffu, toff, i);
-        const uint32_t bhu0 = __shfl_sync(0xffffffffu, hu0, i), btu0 = __shfl_sync(0xffffffffu, tu0, i);
-        for (uint32_t u = bu0 + lane; u < bu1 && !overflow; u += 32) {
-          const uint32_t hs = scaled_shift(bh, u), ts = scaled_shift(bt, u);
-          MetaEntry m;
-          m.op = kMerge;
-          m.a = static_cast<uint16_t>(bho + hs - bhu0);
-          m.b = static_cast<uint16_t>(bto + ts - btu0);
-          m.roll = static_cast<uint16_t>(u - ts);
-          mk[boff + u - bu0] = m;
-        }
-      }
-      // children become the nodes of level k+1: lane l takes child l
-      const uint32_t src_lane = lane >> 1;
-      const bool is_tail = lane & 1;
-      const uint32_t c_ha = __shfl_sync(0xffffffffu, ha, src_lane), c_ta = __shfl_sync(0xffffffffu, ta, src_lane);
-      const uint32_t c_hn = __shfl_sync(0xffffffffu, hn, src_lane), c_tn = __shfl_sync(0xffffffffu, tn, src_lane);
-      const uint32_t c_hu0 = __shfl_sync(0xffffffffu, hu0, src_lane), c_tu0 = __shfl_sync(0xffffffffu, tu0, src_lane);
-      const uint32_t c_hu1 = __shfl_sync(0xffffffffu, hu1, src_lane), c_tu1 = __shfl_sync(0xffffffffu, tu1, src_lane);
-      const uint32_t c_ho = __shfl_sync(0xffffffffu, hoff, src_lane), c_to = __shfl_sync(0xffffffffu, toff, src_lane);
-      na = is_tail ? c_ta : c_ha;
-      nn = is_tail ? c_tn : c_hn;
-      nu0 = is_tail ? c_tu0 : c_hu0;
-      nu1 = is_tail ? c_tu1 : c_hu1;
-      noff = is_tail ? c_to : c_ho;
-      count *= 2;
-      rows = next_rows;
-    }
-    // bottom level K: rows loaded from src
-    MetaEntry* mK = cmeta + K * max_rows;
-    for (uint32_t i = 0; i < count; ++i) {
-      const uint32_t ba = __shfl_sync(0xffffffffu, na, i);
-      const uint32_t bu0 = __shfl_sync(0xffffffffu, nu0, i), bu1 = __shfl_sync(0xffffffffu, nu1, i);
-      const uint32_t boff = __shfl_sync(0xffffffffu, noff, i);
-      for (uint32_t u = bu0 + lane; u < bu1 && !overflow; u += 32) {
-        MetaEntry m;
-        m.op = kLoad;
-        m.a = static_cast<uint16_t>(ba + u);
-        m.b = 0;
-        m.roll = 0;
-        mK[boff + u - bu0] = m;
-      }
-    }
-    if (lane == 0) {
-      counts[0] = s1 - s0;
-      if (overflow) {
-        for (uint32_t k = 0; k <= K; ++k) counts[k] = 0u;
-        atomicOr(p.error, GF_STATUS_SCHEDULE);
-      }
-    }
+    for (int i = 0; i < NB; ++i) v[i] = (i < NB - 1 || last_ok) ? __ldcg(g + 32 * i) : 0.0f;
+    float* o = bottom + q * pitch + lane;
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+      if (i < NB - 1 || last_ok) o[32 * i] = v[i];
   }
+  cp_async_wait_all();
   __syncthreads();
-  float* bufs[2] = {buf0, buf1};
-  // a failed schedule leaves counts at 0: nothing is evaluated
-  eval_level<true>(cmeta + K * max_rows, counts[K], nullptr, bufs[K & 1], p.pitch, src, bins);
-  __syncthreads();
+  uint32_t off = 0;
   for (int k = static_cast<int>(K) - 1; k >= 0; --k) {
-    eval_level<false>(cmeta + k * max_rows, counts[k], bufs[(k + 1) & 1], bufs[k & 1], p.pitch, nullptr, bins);
+    merge_level<NB>(cmeta + off, hb.count[k], ((k + 1) & 1) ? buf1 : buf0, (k & 1) ? buf1 : buf0, pitch, bins);
+    off += hb.count[k];
     __syncthreads();
   }
 }
 
-// Pass boundaries: depth cuts from split_depth down to 0, final pass K levels
-// (or fewer), earlier passes K levels, the remainder at the bottom.
-__device__ __forceinline__ uint32_t cut_after(uint32_t d, uint32_t dS, uint32_t K) {
-  // next (shallower) cut below depth d in the chain dS -> ... -> 0
-  const uint32_t r = dS % K;
-  if (d == dS && r != 0) return dS - r;
-  return d >= K ? d - K : 0;
+// 64-byte header, async (completes at the next cp_async_wait_all)
+__device__ __forceinline__ void load_header(ColBlock* dst, const ColBlock* src) {
+  if (threadIdx.x < 4)
+    cp_async16(reinterpret_cast<uint4*>(dst) + threadIdx.x, reinterpret_cast<const uint4*>(src) + threadIdx.x);
 }
 
-// One (series, task) per cluster (cluster size 1, 2, 4 or 8).
-__global__ void __launch_bounds__(kThreads, 2) ffa_task_kernel(SearchParams p) {
-  extern __shared__ __align__(16) float sm[];
+// One (series, task) per cluster (cluster size 1, 2, 4 or 8); items are
+// task-major so the series of one task run together.  NB = ceil(bins/32)
+// of every task of the launch.
+template <int NB>
+__global__ void __launch_bounds__(kThreads, 2) ffa_search_kernel(SearchParams p) {
   cg::cluster_group cluster = cg::this_cluster();
   const uint32_t cs = cluster.num_blocks();
   const uint32_t rank = cluster.block_rank();
   const uint32_t cid = blockIdx.x / cs;
   const uint32_t nclusters = gridDim.x / cs;
   const uint32_t pitch = p.pitch;
-  float* buf0 = sm;
-  float* buf1 = sm + p.max_rows * pitch;
-  MetaEntry* cmeta = reinterpret_cast<MetaEntry*>(buf1 + p.max_rows * pitch);
-  uint32_t* counts = reinterpret_cast<uint32_t*>(cmeta + (p.levels + 1) * p.max_rows);
+  ColBlock* hdr = reinterpret_cast<ColBlock*>(g_smem);
+  MetaEntry* cmeta = reinterpret_cast<MetaEntry*>(g_smem + 32);
+  float* buf0 = g_smem + p.front;
+  float* buf1 = buf0 + p.max_rows * pitch;
   float* q0 = p.scratch ? p.scratch + static_cast<uint64_t>(cid) * 2 * p.scratch_elems : nullptr;
   float* q1 = q0 ? q0 + p.scratch_elems : nullptr;
   const uint64_t nitems = static_cast<uint64_t>(p.nseries) * p.nitem_tasks;
   for (uint64_t item = cid; item < nitems; item += nclusters) {
-    const uint32_t series = static_cast<uint32_t>(item / p.nitem_tasks);
-    const uint32_t task = p.item_tasks[item % p.nitem_tasks];
+    const uint32_t task = p.item_tasks[item / p.nseries];
+    const uint32_t series = static_cast<uint32_t>(item % p.nseries);
     const TaskDev t = p.tasks[task];
     const float* input = p.prepared + series * p.prep_stride + t.prep_offset;
     const uint32_t bins = t.bins;
@@ -540,21 +557,22 @@ __global__ void __launch_bounds__(kThreads, 2) ffa_task_kernel(SearchParams p) {
     if (dS == 0) {
       // whole task on chip: levels below the root, then root rows in batches
       if (t.rows == 1) {
-        load_rows<false>(input, 1, bins, buf0, pitch);
+        load_rows_async<NB>(input, 1, bins, buf0, pitch);
+        cp_async_wait_all();
         __syncthreads();
-        detect_rows(buf0, pitch, 1, 0, buf1, cp_pitch, da);
+        detect_rows<NB>(buf0, pitch, 1, 0, buf1, cp_pitch, da);
         continue;
       }
-      float* lvl1 = eval_subtree(p, input, t.rows, bins, 1, buf0, buf1);
+      float* lvl1 = eval_subtree<NB>(p, input, t.rows, bins, 1, buf0, buf1, cmeta);
       float* other = lvl1 == buf0 ? buf1 : buf0;
       const uint32_t md = tree_depth(t.rows);
-      const MetaEntry* root = p.sub_meta + p.sub_offset[t.rows] + (md - 1) * t.rows;
+      const MetaEntry* root = cmeta + (md - 1) * t.rows;
       const uint32_t batch = umin32(kThreads, (p.max_rows * pitch) / (pitch + cp_pitch));
       for (uint32_t b0 = 0; b0 < t.rows_eval; b0 += batch) {
         const uint32_t cnt = umin32(batch, t.rows_eval - b0);
-        eval_level<false>(root + b0, cnt, lvl1, other, pitch, nullptr, bins);
+        merge_level<NB>(root + b0, cnt, lvl1, other, pitch, bins);
         __syncthreads();
-        detect_rows(other, pitch, cnt, b0, other + batch * pitch, cp_pitch, da);
+        detect_rows<NB>(other, pitch, cnt, b0, other + batch * pitch, cp_pitch, da);
       }
       continue;
     }
@@ -562,50 +580,37 @@ __global__ void __launch_bounds__(kThreads, 2) ffa_task_kernel(SearchParams p) {
     const uint32_t nsub = 1u << dS;
     for (uint32_t sub = rank; sub < nsub; sub += cs) {
       const Node nd = node_at(sub, t.rows, dS);
-      if (nd.n == 1) {
-        load_rows<false>(input + static_cast<uint64_t>(nd.a) * bins, 1, bins, buf0, pitch);
-        __syncthreads();
-        store_rows(buf0, pitch, 1, bins, q0 + static_cast<uint64_t>(nd.a) * bins);
-      } else {
-        const float* res = eval_subtree(p, input + static_cast<uint64_t>(nd.a) * bins, nd.n, bins, 0, buf0, buf1);
-        store_rows(res, pitch, nd.n, bins, q0 + static_cast<uint64_t>(nd.a) * bins);
-      }
+      const float* res = eval_subtree<NB>(p, input + static_cast<uint64_t>(nd.a) * bins, nd.n, bins, 0, buf0, buf1,
+                                          cmeta);
+      store_rows<NB>(res, pitch, nd.n, bins, q0 + static_cast<uint64_t>(nd.a) * bins);
       __syncthreads();
     }
     cluster.sync();
-    // 2. column passes up to the root
+    // 2. column passes up to the root (the last one fused with detection)
     float* src = q0;
     float* dst = q1;
-    uint32_t d = dS;
-    while (true) {
-      const uint32_t dn = cut_after(d, dS, p.levels);
-      const uint32_t K = d - dn;
-      const bool final_pass = dn == 0;
-      const uint32_t R = final_pass ? p.final_rows : p.block_rows;
-      const uint32_t nnodes = 1u << dn;
-      const uint32_t maxn = (t.rows + nnodes - 1) >> dn;
-      const uint32_t limit = final_pass ? t.rows_eval : maxn;
-      const uint32_t bpn = (limit + R - 1) / R;
-      const uint32_t units = nnodes * bpn;
-      for (uint32_t u = rank; u < units; u += cs) {
-        const Node X = node_at(u / bpn, t.rows, dn);
-        const uint32_t s0 = (u % bpn) * R;
-        const uint32_t s1 = umin32(s0 + R, final_pass ? t.rows_eval : X.n);
-        if (s0 >= s1) continue;
-        eval_column(p, X, s0, s1, K, src, bins, buf0, buf1, cmeta, counts);
-        if (final_pass) {
-          detect_rows(buf0, pitch, counts[0], s0, buf1, cp_pitch, da);
+    for (uint32_t ps = 0; ps < t.npasses; ++ps) {
+      const PassDev pd = p.passes[t.pass_begin + ps];
+      const ColBlock* blocks = p.blocks + pd.block_begin;
+      if (rank < pd.nblocks) load_header(&hdr[0], blocks + rank);
+      cp_async_wait_all();
+      __syncthreads();
+      uint32_t it = 0;
+      for (uint32_t u = rank; u < pd.nblocks; u += cs, ++it) {
+        const ColBlock& hb = hdr[it & 1];
+        if (u + cs < pd.nblocks) load_header(&hdr[(it + 1) & 1], blocks + u + cs);
+        eval_block<NB>(p, hb, src, bins, buf0, buf1, cmeta);
+        if (hb.final_pass) {
+          detect_rows<NB>(buf0, pitch, hb.count[0], hb.out_row, buf1, cp_pitch, da);
         } else {
-          store_rows(buf0, pitch, counts[0], bins, dst + static_cast<uint64_t>(X.a + s0) * bins);
+          store_rows<NB>(buf0, pitch, hb.count[0], bins, dst + static_cast<uint64_t>(hb.out_row) * bins);
           __syncthreads();
         }
       }
       cluster.sync();
-      if (final_pass) break;
       float* tmp = src;
       src = dst;
       dst = tmp;
-      d = dn;
     }
   }
 }
@@ -637,6 +642,18 @@ __global__ void __launch_bounds__(kThreads) ffa_level_kernel(const float* __rest
   }
 }
 
+using SearchKernel = void (*)(SearchParams);
+
+// ffa_search_kernel<NB> for NB = 1 .. 16 (bins <= 512)
+SearchKernel search_kernel_for(uint32_t nb) {
+  static const SearchKernel table[16] = {
+      ffa_search_kernel<1>,  ffa_search_kernel<2>,  ffa_search_kernel<3>,  ffa_search_kernel<4>,
+      ffa_search_kernel<5>,  ffa_search_kernel<6>,  ffa_search_kernel<7>,  ffa_search_kernel<8>,
+      ffa_search_kernel<9>,  ffa_search_kernel<10>, ffa_search_kernel<11>, ffa_search_kernel<12>,
+      ffa_search_kernel<13>, ffa_search_kernel<14>, ffa_search_kernel<15>, ffa_search_kernel<16>};
+  return table[nb - 1];
+}
+
 }  // namespace
 }  // namespace gf
 
@@ -644,10 +661,11 @@ using namespace gf;
 
 struct FfaClass {
   int cluster = 1;             // CTAs cooperating on one (series, task)
-  std::vector<uint32_t> tasks;
+  uint32_t nb = 1;             // ceil(bins / 32) of every task of the class
+  SearchKernel kernel = nullptr;
+  std::vector<uint32_t> tasks; // largest first
   uint64_t max_elems = 0;      // rows * bins of the largest task (scratch per cluster)
   int nclusters = 0;           // resident clusters
-  uint64_t scratch_offset = 0; // floats into the program scratch
   DeviceBlob tasks_d;
 };
 
@@ -660,16 +678,19 @@ struct gf_ffa_program {
   std::vector<OctaveDev> octaves;
   std::vector<MetaEntry> sub_meta;
   std::vector<uint32_t> sub_offset;
+  std::vector<MetaEntry> col_meta;
+  std::vector<ColBlock> blocks;
+  std::vector<PassDev> passes;
   std::vector<FfaClass> classes;
   uint64_t nsamples = 0;
   uint64_t prep_stride = 0;
   uint32_t max_bins = 0, max_width = 0;
-  uint32_t pitch = 0, max_rows = 0, block_rows = 0, final_rows = 0, levels = 0;
+  uint32_t pitch = 0, max_rows = 0, block_rows = 0, final_rows = 0, levels = 0, front = 0;
   uint64_t halo = 0;
   uint64_t max_series = 0;
   uint64_t scratch_floats = 0;
   size_t smem_bytes = 0;
-  DeviceBlob tasks_d, trials_d, octaves_d, sub_meta_d, sub_offset_d;
+  DeviceBlob tasks_d, trials_d, octaves_d, sub_meta_d, sub_offset_d, col_meta_d, blocks_d, passes_d;
 };
 
 namespace {
@@ -760,6 +781,115 @@ void build_subtree_schedule(uint32_t n, std::vector<MetaEntry>& out) {
   }
 }
 
+// Pass boundaries: depth cuts from split_depth down to 0; the first pass
+// takes split_depth mod K levels (when non-zero), the others K levels.
+uint32_t cut_after(uint32_t d, uint32_t dS, uint32_t K) {
+  const uint32_t r = dS % K;
+  if (d == dS && r != 0) return dS - r;
+  return d >= K ? d - K : 0;
+}
+
+// IEEE single arithmetic of ffa.cpp:153-171 (host code is built without
+// contraction, so this matches the device's _rn intrinsics bit for bit)
+float host_shift_scale(uint32_t part, uint32_t n) {
+  return static_cast<float>(part - 1) / static_cast<float>(n - 1);
+}
+uint32_t host_scaled_shift(float scale, uint32_t s) {
+  const float x = scale * static_cast<float>(s);
+  return static_cast<uint32_t>(x + 0.5f);
+}
+
+struct ColumnNode {
+  uint32_t a, n, u0, u1, off;  // task rows [a, a+n); rows [u0, u1) of it; buffer row of u0
+};
+
+// Column block: rows [s0, s1) of node X (task rows [xa, xa+xn)) from the rows
+// K levels down.  Level k+1 holds, for every node of level k, the head- and
+// tail-child rows its rows read (the index arithmetic of ffa.cpp), so each
+// level stays within max_rows rows.
+void build_column_block(uint32_t bins, uint32_t xa, uint32_t xn, uint32_t s0, uint32_t s1, uint32_t K,
+                        uint32_t max_rows, bool final_pass, std::vector<MetaEntry>& meta,
+                        std::vector<ColBlock>& blocks) {
+  ColBlock b{};
+  b.levels = static_cast<uint8_t>(K);
+  b.final_pass = final_pass ? 1 : 0;
+  b.out_row = final_pass ? s0 : xa + s0;
+  b.count[0] = static_cast<uint16_t>(s1 - s0);
+  std::vector<ColumnNode> nodes{ColumnNode{xa, xn, s0, s1, 0}};
+  std::vector<std::vector<MetaEntry>> level(K);
+  for (uint32_t k = 0; k < K; ++k) {
+    std::vector<ColumnNode> children;
+    uint32_t off = 0;
+    for (const ColumnNode& nd : nodes) {
+      check_arg(nd.n >= 2, "FFA column schedule reached a one-row node");
+      const uint32_t h = nd.n / 2, t = nd.n - h;
+      const float hsc = host_shift_scale(h, nd.n), tsc = host_shift_scale(t, nd.n);
+      ColumnNode hc{nd.a, h, host_scaled_shift(hsc, nd.u0), host_scaled_shift(hsc, nd.u1 - 1) + 1, off};
+      off += hc.u1 - hc.u0;
+      ColumnNode tc{nd.a + h, t, host_scaled_shift(tsc, nd.u0), host_scaled_shift(tsc, nd.u1 - 1) + 1, off};
+      off += tc.u1 - tc.u0;
+      for (uint32_t u = nd.u0; u < nd.u1; ++u) {
+        const uint32_t hs = host_scaled_shift(hsc, u), ts = host_scaled_shift(tsc, u);
+        MetaEntry m{};
+        m.op = kMerge;
+        m.a = static_cast<uint16_t>(hc.off + hs - hc.u0);
+        m.b = static_cast<uint16_t>(tc.off + ts - tc.u0);
+        m.roll = static_cast<uint16_t>((u - ts) % bins);
+        level[k].push_back(m);
+      }
+      children.push_back(hc);
+      children.push_back(tc);
+    }
+    check_arg(off <= max_rows, "FFA column schedule exceeds the shared-memory tile");
+    for (const MetaEntry& m : level[k])
+      check_arg(m.a < off && m.b < off && m.roll < bins, "FFA column schedule entry out of range");
+    b.count[k + 1] = static_cast<uint16_t>(off);
+    nodes.swap(children);
+  }
+  check_arg(nodes.size() <= 8, "FFA column block has too many bottom runs");
+  b.nruns = static_cast<uint8_t>(nodes.size());
+  for (size_t j = 0; j < nodes.size(); ++j) {
+    check_arg(nodes[j].u0 < nodes[j].u1 && nodes[j].u1 <= nodes[j].n, "FFA column run out of range");
+    b.run_off[j] = static_cast<uint16_t>(nodes[j].off);
+    b.run_row[j] = static_cast<uint16_t>(nodes[j].a + nodes[j].u0);
+  }
+  if (meta.size() & 1) meta.push_back(MetaEntry{});
+  b.meta = static_cast<uint32_t>(meta.size());
+  for (int k = static_cast<int>(K) - 1; k >= 0; --k) meta.insert(meta.end(), level[k].begin(), level[k].end());
+  if (meta.size() & 1) meta.push_back(MetaEntry{});
+  blocks.push_back(b);
+}
+
+// All column passes of a task split at depth dS (> 0).
+void build_task_passes(gf_ffa_program& P, TaskDev& d) {
+  const uint32_t dS = d.split_depth, K = P.levels;
+  d.pass_begin = static_cast<uint32_t>(P.passes.size());
+  uint32_t depth = dS;
+  while (true) {
+    const uint32_t dn = cut_after(depth, dS, K);
+    const uint32_t levels = depth - dn;
+    const bool final_pass = dn == 0;
+    const uint32_t R = final_pass ? P.final_rows : P.block_rows;
+    const uint32_t nnodes = 1u << dn;
+    const uint32_t maxn = (d.rows + nnodes - 1) >> dn;
+    const uint32_t limit = final_pass ? d.rows_eval : maxn;
+    const uint32_t bpn = (limit + R - 1) / R;
+    PassDev pd{static_cast<uint32_t>(P.blocks.size()), 0u};
+    for (uint32_t u = 0; u < nnodes * bpn; ++u) {
+      const Node X = node_at(u / bpn, d.rows, dn);
+      const uint32_t s0 = (u % bpn) * R;
+      const uint32_t s1 = std::min<uint32_t>(s0 + R, final_pass ? d.rows_eval : X.n);
+      if (s0 >= s1) continue;
+      build_column_block(d.bins, X.a, X.n, s0, s1, levels, P.max_rows, final_pass, P.col_meta, P.blocks);
+    }
+    pd.nblocks = static_cast<uint32_t>(P.blocks.size()) - pd.block_begin;
+    P.passes.push_back(pd);
+    if (final_pass) break;
+    depth = dn;
+  }
+  d.npasses = static_cast<uint32_t>(P.passes.size()) - d.pass_begin;
+}
+
 }  // namespace
 
 extern "C" int gf_downsampled_size(uint64_t n, double factor, uint64_t* out) {
@@ -820,24 +950,28 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
       P->max_bins = std::max<uint32_t>(P->max_bins, static_cast<uint32_t>(t.bins));
     }
     for (uint64_t w : P->widths) P->max_width = std::max<uint32_t>(P->max_width, static_cast<uint32_t>(w));
-    // shared-memory geometry: two row buffers of max_rows rows, the column
-    // schedules, sized for two CTAs per SM where possible
+    // shared-memory geometry: two ColBlock headers, the staged schedule, two
+    // row buffers of max_rows rows; sized for two CTAs per SM
     P->pitch = P->max_bins | 1u;
     P->levels = 3;
     const size_t budget = 110 * 1024;
-    auto smem_for = [&](uint32_t rows, uint32_t K) {
-      return 2ull * rows * P->pitch * 4 + (K + 1ull) * rows * sizeof(MetaEntry) + 64;
+    auto front_for = [&](uint32_t rows) {
+      const uint64_t meta_cap = std::max<uint64_t>(static_cast<uint64_t>(tree_depth(rows)) * rows,
+                                                   static_cast<uint64_t>(P->levels) * rows + 2);
+      return static_cast<uint32_t>(round_up(std::max<uint64_t>(32 + 2 * meta_cap, P->max_bins), 4));
     };
+    auto smem_for = [&](uint32_t rows) { return (front_for(rows) + 2ull * rows * P->pitch) * 4; };
     uint32_t rows = 8;
-    while (smem_for(rows + 1, P->levels) <= budget) ++rows;
+    while (smem_for(rows + 1) <= budget) ++rows;
     P->max_rows = rows;
+    P->front = front_for(rows);
     // R + 3 (2^K - 1) rows at the bottom of a column
     while (P->levels > 1 && static_cast<int>(rows) - 3 * ((1 << P->levels) - 1) < 8) --P->levels;
     P->block_rows = rows - 3 * ((1u << P->levels) - 1);
     const uint32_t cp_pitch = (P->max_bins + P->max_width + 2) | 1u;
     P->final_rows = std::min<uint32_t>(P->block_rows, (rows * P->pitch) / cp_pitch);
     check_arg(P->final_rows >= 1 && P->block_rows >= 1, "FFA bins too large for the shared-memory tiles");
-    P->smem_bytes = smem_for(rows, P->levels);
+    P->smem_bytes = smem_for(rows);
     // subtree schedules for every size up to max_rows
     P->sub_offset.assign(rows + 1, 0u);
     for (uint32_t n = 1; n <= rows; ++n) {
@@ -845,8 +979,8 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
       build_subtree_schedule(n, P->sub_meta);
     }
     if (P->sub_meta.empty()) P->sub_meta.push_back(MetaEntry{});
-    // tasks, trials and classes
-    std::map<int, size_t> class_of;
+    // tasks, trials, column schedules and classes
+    std::map<std::pair<int, uint32_t>, size_t> class_of;
     for (uint64_t i = 0; i < ntasks; ++i) {
       const auto& t = P->tasks[i];
       for (uint64_t w : P->widths)
@@ -872,34 +1006,45 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
       while (ceil_div(t.rows, 1ull << ds) > rows) ++ds;
       check_arg(ds <= 15, "FFA task too deep");
       d.split_depth = ds;
+      if (ds > 0) build_task_passes(*P, d);
       P->task_dev.push_back(d);
+      // cluster sized by rows for split tasks; on-chip tasks use key 0
       int cluster = 1;
       if (ds > 0) {
-        cluster = 0;  // medium and large tasks: scratch; cluster sized by rows
-        const uint64_t per = 512;
-        int c = 1;
-        while (c < kClusterSize && static_cast<uint64_t>(c) * per < t.rows) c *= 2;
-        cluster = c;
+        while (cluster < kClusterSize && static_cast<uint64_t>(cluster) * 512 < t.rows) cluster *= 2;
       }
-      // class key: 0 = on-chip (no scratch), else the cluster size
-      const int key = ds == 0 ? 0 : cluster;
+      const uint32_t nb = static_cast<uint32_t>(ceil_div(t.bins, 32));
+      const std::pair<int, uint32_t> key{ds == 0 ? 0 : cluster, nb};
       if (!class_of.count(key)) {
         class_of[key] = P->classes.size();
         P->classes.emplace_back();
-        P->classes.back().cluster = ds == 0 ? 1 : cluster;
+        P->classes.back().cluster = cluster;
+        P->classes.back().nb = nb;
+        P->classes.back().kernel = search_kernel_for(nb);
       }
       FfaClass& c = P->classes[class_of[key]];
       c.tasks.push_back(static_cast<uint32_t>(i));
       if (ds > 0) c.max_elems = std::max<uint64_t>(c.max_elems, t.rows * t.bins);
     }
-    cuda_check(cudaFuncSetAttribute(ffa_task_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(P->smem_bytes)),
-               "cudaFuncSetAttribute(ffa_task_kernel)");
-    cuda_check(cudaFuncSetAttribute(ffa_task_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
-               "cudaFuncSetAttribute(cluster size)");
+    // launch order: widest clusters (longest items) first
+    std::stable_sort(P->classes.begin(), P->classes.end(), [](const FfaClass& x, const FfaClass& y) {
+      return x.cluster != y.cluster ? x.cluster > y.cluster : x.nb > y.nb;
+    });
+    if (P->col_meta.empty()) P->col_meta.resize(2);
+    if (P->blocks.empty()) P->blocks.resize(1);
+    if (P->passes.empty()) P->passes.resize(1);
     int sms = 0;
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_id), "device attribute");
     for (auto& c : P->classes) {
+      // largest tasks first so long items start early
+      std::stable_sort(c.tasks.begin(), c.tasks.end(), [&](uint32_t x, uint32_t y) {
+        return P->tasks[x].rows * P->tasks[x].bins > P->tasks[y].rows * P->tasks[y].bins;
+      });
+      cuda_check(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(P->smem_bytes)),
+                 "cudaFuncSetAttribute(ffa_search_kernel)");
+      cuda_check(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+                 "cudaFuncSetAttribute(cluster size)");
       cudaLaunchConfig_t cfg{};
       cfg.gridDim = dim3(c.cluster, 1, 1);
       cfg.blockDim = dim3(kThreads, 1, 1);
@@ -912,13 +1057,11 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
       cfg.attrs = &attr;
       cfg.numAttrs = 1;
       int n = 0;
-      cuda_check(cudaOccupancyMaxActiveClusters(&n, ffa_task_kernel, &cfg), "cudaOccupancyMaxActiveClusters");
+      cuda_check(cudaOccupancyMaxActiveClusters(&n, c.kernel, &cfg), "cudaOccupancyMaxActiveClusters");
       check_arg(n > 0, "FFA kernel cannot be resident on this device");
       c.nclusters = n;
-      if (c.max_elems) {
-        c.scratch_offset = P->scratch_floats;
-        P->scratch_floats += static_cast<uint64_t>(n) * 2 * c.max_elems;
-      }
+      // classes run one after another on the stream: they share the scratch
+      P->scratch_floats = std::max<uint64_t>(P->scratch_floats, static_cast<uint64_t>(n) * 2 * c.max_elems);
       c.tasks_d.upload(c.tasks.data(), c.tasks.size() * sizeof(uint32_t), device_id);
     }
     P->tasks_d.upload(P->task_dev.data(), P->task_dev.size() * sizeof(TaskDev), device_id);
@@ -926,6 +1069,9 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
     P->octaves_d.upload(P->octaves.data(), P->octaves.size() * sizeof(OctaveDev), device_id);
     P->sub_meta_d.upload(P->sub_meta.data(), P->sub_meta.size() * sizeof(MetaEntry), device_id);
     P->sub_offset_d.upload(P->sub_offset.data(), P->sub_offset.size() * sizeof(uint32_t), device_id);
+    P->col_meta_d.upload(P->col_meta.data(), P->col_meta.size() * sizeof(MetaEntry), device_id);
+    P->blocks_d.upload(P->blocks.data(), P->blocks.size() * sizeof(ColBlock), device_id);
+    P->passes_d.upload(P->passes.data(), P->passes.size() * sizeof(PassDev), device_id);
     *out = P.release();
   });
 }
@@ -946,7 +1092,7 @@ extern "C" int gf_ffa_program_info(const gf_ffa_program* P, gf_ffa_info* info) {
     for (const auto& t : P->tasks) mx = std::max<uint64_t>(mx, t.rows * t.bins);
     info->max_task_elements = mx;
     info->metadata_bytes = P->tasks_d.bytes + P->trials_d.bytes + P->octaves_d.bytes + P->sub_meta_d.bytes +
-                           P->sub_offset_d.bytes;
+                           P->sub_offset_d.bytes + P->col_meta_d.bytes + P->blocks_d.bytes + P->passes_d.bytes;
     for (const auto& c : P->classes) info->metadata_bytes += c.tasks_d.bytes;
     info->nclasses = P->classes.size();
   });
@@ -996,18 +1142,16 @@ extern "C" int gf_ffa_search(gf_ffa_program* P, const float* dev_prepared, uint6
     sp.peaks = dev_peaks;
     sp.capacity = capacity;
     sp.counters = reinterpret_cast<unsigned long long*>(dev_counters);
+    sp.col_meta = P->col_meta_d.as<MetaEntry>();
+    sp.blocks = P->blocks_d.as<ColBlock>();
+    sp.passes = P->passes_d.as<PassDev>();
     sp.pitch = P->pitch;
     sp.max_rows = P->max_rows;
-    sp.block_rows = P->block_rows;
-    sp.final_rows = P->final_rows;
-    sp.levels = P->levels;
-    sp.error = reinterpret_cast<uint32_t*>(dev_counters + 1);
-    // largest tasks first so the long clusters start early
-    for (auto it = P->classes.rbegin(); it != P->classes.rend(); ++it) {
-      const FfaClass& c = *it;
+    sp.front = P->front;
+    sp.scratch = static_cast<float*>(dev_scratch);
+    for (const FfaClass& c : P->classes) {
       sp.item_tasks = c.tasks_d.as<uint32_t>();
       sp.nitem_tasks = static_cast<uint32_t>(c.tasks.size());
-      sp.scratch = c.max_elems ? static_cast<float*>(dev_scratch) + c.scratch_offset : nullptr;
       sp.scratch_elems = c.max_elems;
       const uint64_t items = nseries * c.tasks.size();
       const unsigned nclusters = static_cast<unsigned>(std::min<uint64_t>(items, static_cast<uint64_t>(c.nclusters)));
@@ -1023,7 +1167,7 @@ extern "C" int gf_ffa_search(gf_ffa_program* P, const float* dev_prepared, uint6
       attr.val.clusterDim.z = 1;
       cfg.attrs = &attr;
       cfg.numAttrs = 1;
-      cuda_check(cudaLaunchKernelEx(&cfg, ffa_task_kernel, sp), "ffa_task_kernel launch");
+      cuda_check(cudaLaunchKernelEx(&cfg, c.kernel, sp), "ffa_search_kernel launch");
     }
   });
 }
