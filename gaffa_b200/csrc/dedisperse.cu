@@ -13,7 +13,10 @@
 // 1008 consecutive output samples (252 output words of 4 samples).  The CTA
 // streams channel chunks: for each channel it copies the window
 // [t0 + base, t0 + base + RS) (base = delay of the block's first DM rounded down
-// to 16) into shared memory with 16-byte loads.  A warp reads its DM's shifted
+// to 16) into shared memory with 16-byte cp.async copies, double-buffered so
+// chunk k+1 lands while chunk k is summed.  DM blocks are the fastest grid
+// index, so the CTAs resident at one time cover a few time tiles of every DM
+// block of the launch and read each input window from L2.  A warp reads its DM's shifted
 // window as aligned 32-bit words: the delay offset off = d - base splits into a
 // word offset q = off >> 2 and a byte class s = off & 3.  The host sorts each
 // warp's channels by class, so the class is static inside the loop: a word
@@ -66,6 +69,7 @@ struct BytesParams {
   const uint32_t* records;   // + g*rec_group_stride + dm*rec_dm_stride + chunk*record_words
   uint64_t rec_group_stride;
   uint64_t rec_dm_stride;
+  int nblocks;               // DM blocks per group in the launch (fastest grid index)
   int dm_count;              // DMs per group handled by the launch
   int dm_count_last;         // DMs of the launch's last group
   int ngroups;
@@ -138,12 +142,21 @@ __device__ __forceinline__ void accumulate_class(const uint32_t* __restrict__ sm
   pos += npairs;
 }
 
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 template <typename OutT>
 __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesParams p) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int group = blockIdx.z;
-  const int block = blockIdx.y;
-  const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * p.cta_samples;
+  // DM block fastest: the CTAs resident at once share their input windows in L2
+  const int block = static_cast<int>(blockIdx.x % static_cast<unsigned>(p.nblocks));
+  const uint64_t t0 = static_cast<uint64_t>(blockIdx.x / static_cast<unsigned>(p.nblocks)) * p.cta_samples;
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int dm_sub = warp / p.warps_per_dm;
@@ -153,15 +166,56 @@ __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesPara
   const bool active = dm_sub < p.dms_per_cta && dm_local < dm_limit;
 
   const int group_rows = min(p.rows_per_group, p.total_rows - group * p.rows_per_group);
-  uint8_t* rows = smem;
-  uint32_t* rec_smem = reinterpret_cast<uint32_t*>(smem + (p.chunk_rows + 1) * p.row_bytes);
-  const uint32_t* smem_words = reinterpret_cast<const uint32_t*>(smem);
+  // two stage buffers: chunk rows + a zero row, then the chunk's records
+  const uint32_t rows_bytes = static_cast<uint32_t>(p.chunk_rows + 1) * p.row_bytes;
+  const uint32_t buf_bytes = rows_bytes + static_cast<uint32_t>(p.dms_per_cta * p.record_words) * 4u;
   const uint8_t* in_group = p.in + group * p.in_group_stride;
   const int32_t* base = p.base + group * p.base_group_stride + static_cast<uint64_t>(block) * p.rows_per_group;
 
-  // zero row (index chunk_rows) for class padding entries
-  for (int i = threadIdx.x; i < p.row_bytes / 16; i += kThreads)
-    reinterpret_cast<uint4*>(rows + p.chunk_rows * p.row_bytes)[i] = make_uint4(0, 0, 0, 0);
+  // zero rows (class padding entries point at them)
+  for (int i = threadIdx.x; i < 2 * (p.row_bytes / 16); i += kThreads) {
+    const int b = i / (p.row_bytes / 16), v = i % (p.row_bytes / 16);
+    reinterpret_cast<uint4*>(smem + b * buf_bytes + p.chunk_rows * p.row_bytes)[v] = make_uint4(0, 0, 0, 0);
+  }
+
+  // chunk k's channel windows and records into buffer b (async where in range)
+  auto stage = [&](int k, int b) {
+    uint8_t* rows = smem + b * buf_bytes;
+    uint32_t* rec_smem = reinterpret_cast<uint32_t*>(rows + rows_bytes);
+    const int row0 = k * p.chunk_rows;
+    const int nrows = min(p.chunk_rows, group_rows - row0);
+    const int vecs_per_row = p.row_bytes / 16;
+    for (int i = threadIdx.x; i < nrows * vecs_per_row; i += kThreads) {
+      const int r = i / vecs_per_row;
+      const int v = i - r * vecs_per_row;
+      const uint64_t t = t0 + static_cast<uint64_t>(base[row0 + r]) + 16ull * v;
+      const uint8_t* src = in_group + static_cast<uint64_t>(row0 + r) * p.in_row_stride + t;
+      uint8_t* dst = rows + r * p.row_bytes + 16 * v;
+      if (t + 16 <= p.in_valid) {
+        cp_async16(dst, src);
+      } else {
+        uint8_t tmp[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) tmp[j] = (t + j < p.in_valid) ? src[j] : 0;
+        uint4 val;
+        memcpy(&val, tmp, 16);
+        *reinterpret_cast<uint4*>(dst) = val;
+      }
+    }
+    const int vecs_per_rec = p.record_words / 4;
+    for (int i = threadIdx.x; i < p.dms_per_cta * vecs_per_rec; i += kThreads) {
+      const int d = i / vecs_per_rec;
+      const int w = 4 * (i - d * vecs_per_rec);
+      const int dl = block * p.dms_per_cta + d;
+      uint32_t* dst = rec_smem + d * p.record_words + w;
+      if (dl < dm_limit) {
+        cp_async16(dst, p.records + group * p.rec_group_stride + dl * p.rec_dm_stride +
+                            static_cast<uint64_t>(k) * p.record_words + w);
+      } else {
+        *reinterpret_cast<uint4*>(dst) = make_uint4(0, 0, 0, 0);
+      }
+    }
+  };
 
   uint32_t e[4][kWords], o[4][kWords], acc[kWords][4];
 #pragma unroll
@@ -174,41 +228,21 @@ __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesPara
   const int lane_word = sub * kOutWords + lane;
   const int chunks_per_flush = kFlushChannels / p.chunk_rows;
 
+  stage(0, 0);
+  cp_async_commit();
   for (int k = 0; k < p.nchunks; ++k) {
-    const int row0 = k * p.chunk_rows;
-    const int nrows = min(p.chunk_rows, group_rows - row0);
-    __syncthreads();
-    // stage the chunk's channel windows
-    const int vecs_per_row = p.row_bytes / 16;
-    for (int i = threadIdx.x; i < nrows * vecs_per_row; i += kThreads) {
-      const int r = i / vecs_per_row;
-      const int v = i - r * vecs_per_row;
-      const uint64_t t = t0 + static_cast<uint64_t>(base[row0 + r]) + 16ull * v;
-      const uint8_t* src = in_group + static_cast<uint64_t>(row0 + r) * p.in_row_stride + t;
-      uint4 val;
-      if (t + 16 <= p.in_valid) {
-        val = __ldg(reinterpret_cast<const uint4*>(src));
-      } else {
-        uint8_t tmp[16];
-#pragma unroll
-        for (int b = 0; b < 16; ++b) tmp[b] = (t + b < p.in_valid) ? src[b] : 0;
-        memcpy(&val, tmp, 16);
-      }
-      reinterpret_cast<uint4*>(rows + r * p.row_bytes)[v] = val;
-    }
-    for (int i = threadIdx.x; i < p.dms_per_cta * p.record_words; i += kThreads) {
-      const int d = i / p.record_words;
-      const int w = i - d * p.record_words;
-      const int dl = block * p.dms_per_cta + d;
-      uint32_t val = 0u;
-      if (dl < dm_limit)
-        val = p.records[group * p.rec_group_stride + dl * p.rec_dm_stride +
-                        static_cast<uint64_t>(k) * p.record_words + w];
-      rec_smem[i] = val;
+    if (k + 1 < p.nchunks) {
+      stage(k + 1, (k + 1) & 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
     if (active) {
-      const uint32_t* rec = rec_smem + dm_sub * p.record_words;
+      const uint8_t* rows = smem + (k & 1) * buf_bytes;
+      const uint32_t* smem_words = reinterpret_cast<const uint32_t*>(rows);
+      const uint32_t* rec = reinterpret_cast<const uint32_t*>(rows + rows_bytes) + dm_sub * p.record_words;
       const uint32_t counts = rec[0];
       int pos = 1;
       accumulate_class<0>(smem_words, rec, pos, (counts & 0xffu) >> 1, lane_word, e[0], o[0]);
@@ -222,6 +256,7 @@ __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesPara
         flush_class<3>(e[3], o[3], acc, lane);
       }
     }
+    __syncthreads();  // buffer k & 1 is restaged for chunk k + 2
   }
   if (!active) return;
   OutT* out = static_cast<OutT*>(p.out) +
@@ -386,7 +421,7 @@ Launch choose_launch(F&& max_off_for) {
       const int row_bytes = static_cast<int>(round_up(max_off + 4 * ((wpd - 1) * kOutWords + 32 * kWords), 16));
       for (int cr : {64, 32, 16, 8}) {
         const size_t rec = static_cast<size_t>(dpc) * round_up(1 + (cr + 4) / 2, 4) * 4;
-        const size_t smem = static_cast<size_t>(cr + 1) * row_bytes + rec;
+        const size_t smem = 2 * (static_cast<size_t>(cr + 1) * row_bytes + rec);  // double-buffered
         if (smem <= budget && static_cast<size_t>(cr + 1) * row_bytes < 262144) {
           return Launch{dpc, wpd, cr, row_bytes, smem};
         }
@@ -474,8 +509,10 @@ struct BytesStage {
     p.out_group_rows = out_group_rows;
     p.nout = nout;
     const int dmax = std::max(dm_count, dm_count_last);
-    dim3 grid(static_cast<unsigned>(ceil_div(nout, p.cta_samples)),
-              static_cast<unsigned>(ceil_div(dmax, launch.dms_per_cta)), static_cast<unsigned>(gcount));
+    p.nblocks = static_cast<int>(ceil_div(dmax, launch.dms_per_cta));
+    const uint64_t ctas = ceil_div(nout, p.cta_samples) * static_cast<uint64_t>(p.nblocks);
+    if (ctas >= (1ull << 31)) raise(GF_EINVAL, "dedispersion launch too large");
+    dim3 grid(static_cast<unsigned>(ctas), 1u, static_cast<unsigned>(gcount));
     auto kernel = dedisperse_bytes_kernel<OutT>;
     cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(launch.smem)),
