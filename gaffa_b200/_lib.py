@@ -78,6 +78,16 @@ class CandidateOptions(C.Structure):
                 ("cluster_across_widths", i32), ("reserved", i32), ("max_candidates", u64)]
 
 
+class HarmonicContext(C.Structure):
+    _fields_ = [("observation_seconds", dbl), ("frequency_low_mhz", dbl), ("frequency_high_mhz", dbl)]
+
+
+class HarmonicOptions(C.Structure):
+    _fields_ = [("max_harmonic", u64), ("denominator_max", u64), ("frequency_tolerance_bins", dbl),
+                ("phase_distance_max", dbl), ("dm_distance_max", dbl), ("use_snr_consistency", i32),
+                ("reserved", i32), ("snr_distance_max", dbl)]
+
+
 class SynthPulsar(C.Structure):
     _fields_ = [("period", dbl), ("dm", dbl), ("duty_cycle", dbl), ("amplitude", dbl), ("phase", dbl)]
 
@@ -104,6 +114,12 @@ CAND_DTYPE = np.dtype([
     ("duty_cycle", "<f8"), ("snr", "<f4"), ("reserved", "<u4"), ("peak_count", "<u8"),
     ("dm_index_min", "<u8"), ("dm_index_max", "<u8"), ("frequency_min", "<f8"),
     ("frequency_max", "<f8"), ("best_peak", PEAK_DTYPE)])
+
+HARMONIC_DTYPE = np.dtype([
+    ("is_harmonic", "<i4"), ("reserved", "<i4"), ("parent_index", "<u8"), ("numerator", "<i4"),
+    ("denominator", "<i4"), ("frequency_error_bins", "<f8"), ("phase_distance", "<f8"),
+    ("dm_distance", "<f8"), ("expected_snr", "<f8"), ("snr_distance", "<f8")])
+NO_HARMONIC_PARENT = (1 << 64) - 1
 
 assert C.sizeof(FfaTask) == TASK_DTYPE.itemsize == 72
 assert PEAK_RECORD_DTYPE.itemsize == 24 and PEAK_DTYPE.itemsize == 96
@@ -142,6 +158,8 @@ _SIGNATURES = [
     ("gf_synth_generate", C.c_int, [C.POINTER(SynthDesc), u64, u64, vp, vp]),
     ("gf_fold_noalloc_max_bytes", u64, []),
     ("gf_fold_time_series_noalloc", C.c_int, [vp, i32, u64, dbl, dbl, u64, u64, vp, vp, vp, vp]),
+    ("gf_flag_harmonics", C.c_int, [vp, u64, C.POINTER(HarmonicContext), C.POINTER(HarmonicOptions), vp, vp]),
+    ("gf_remove_harmonics", C.c_int, [vp, vp, u64, u64, vp, C.POINTER(u64)]),
 ]
 
 ENTRY_POINTS = [name for name, _, _ in _SIGNATURES]

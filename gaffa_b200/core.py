@@ -371,6 +371,42 @@ def select_candidates(peaks: np.ndarray, observation_seconds: float, frequency_c
     return out
 
 
+def harmonic_options(max_harmonic: int = 16, denominator_max: int = 5, frequency_tolerance_bins: float = 1.5,
+                     phase_distance_max: float = 1.0, dm_distance_max: float = 3.0,
+                     use_snr_consistency: bool = False, snr_distance_max: float = 3.0):
+    """HarmonicOptions (include/gaffa/harmonic.h:22-36) with its defaults."""
+    return _lib.HarmonicOptions(max_harmonic, denominator_max, frequency_tolerance_bins, phase_distance_max,
+                                dm_distance_max, int(use_snr_consistency), 0, snr_distance_max)
+
+
+def flag_harmonics(candidates: np.ndarray, observation_seconds: float, frequency_low_mhz: float,
+                   frequency_high_mhz: float, options=None) -> tuple[np.ndarray, np.ndarray]:
+    """flag_harmonics_cpu (src/gaffa/harmonic.cpp:245-292): the candidates in
+    harmonic ranking order and their relations (HARMONIC_DTYPE)."""
+    candidates = np.ascontiguousarray(candidates, _lib.CAND_DTYPE)
+    ctx = _lib.HarmonicContext(observation_seconds, frequency_low_mhz, frequency_high_mhz)
+    opts = options if options is not None else harmonic_options()
+    out = np.zeros(len(candidates), _lib.CAND_DTYPE)
+    rel = np.zeros(len(candidates), _lib.HARMONIC_DTYPE)
+    check(_lib.lib().gf_flag_harmonics(ptr(candidates), len(candidates), C.byref(ctx), C.byref(opts),
+                                       ptr(out) if len(out) else None, ptr(rel) if len(rel) else None))
+    return out, rel
+
+
+def remove_harmonics(sorted_candidates: np.ndarray, relations: np.ndarray, max_candidates: int = 0) -> np.ndarray:
+    """remove_harmonics_cpu (src/gaffa/harmonic.cpp:294-309)."""
+    sorted_candidates = np.ascontiguousarray(sorted_candidates, _lib.CAND_DTYPE)
+    relations = np.ascontiguousarray(relations, _lib.HARMONIC_DTYPE)
+    if len(sorted_candidates) != len(relations):
+        raise ValueError("candidates and relations must have the same length")
+    out = np.zeros(len(sorted_candidates), _lib.CAND_DTYPE)
+    n = _lib.u64()
+    check(_lib.lib().gf_remove_harmonics(ptr(sorted_candidates) if len(out) else None,
+                                         ptr(relations) if len(out) else None, len(out), max_candidates,
+                                         ptr(out) if len(out) else None, C.byref(n)))
+    return out[: n.value]
+
+
 # ---------------------------------------------------------------------------
 # folding
 # ---------------------------------------------------------------------------

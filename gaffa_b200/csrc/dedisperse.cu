@@ -64,7 +64,7 @@ struct BytesParams {
   uint64_t in_valid;         // valid samples per row (zero beyond)
   int rows_per_group;
   int total_rows;            // group g has min(rows_per_group, total_rows - g*rows_per_group) rows
-  const int32_t* base;       // + g*base_group_stride + blockIdx.y*rows_per_group
+  const int32_t* base;       // + g*base_group_stride + dm_block*rows_per_group
   uint64_t base_group_stride;
   const uint32_t* records;   // + g*rec_group_stride + dm*rec_dm_stride + chunk*record_words
   uint64_t rec_group_stride;
@@ -184,22 +184,24 @@ __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesPara
     uint32_t* rec_smem = reinterpret_cast<uint32_t*>(rows + rows_bytes);
     const int row0 = k * p.chunk_rows;
     const int nrows = min(p.chunk_rows, group_rows - row0);
+    // a warp per channel row, lanes over its 16-byte vectors
     const int vecs_per_row = p.row_bytes / 16;
-    for (int i = threadIdx.x; i < nrows * vecs_per_row; i += kThreads) {
-      const int r = i / vecs_per_row;
-      const int v = i - r * vecs_per_row;
-      const uint64_t t = t0 + static_cast<uint64_t>(base[row0 + r]) + 16ull * v;
-      const uint8_t* src = in_group + static_cast<uint64_t>(row0 + r) * p.in_row_stride + t;
-      uint8_t* dst = rows + r * p.row_bytes + 16 * v;
-      if (t + 16 <= p.in_valid) {
-        cp_async16(dst, src);
-      } else {
-        uint8_t tmp[16];
+    for (int r = warp; r < nrows; r += kWarps) {
+      const uint64_t t_row = t0 + static_cast<uint64_t>(base[row0 + r]);
+      const uint8_t* src_row = in_group + static_cast<uint64_t>(row0 + r) * p.in_row_stride + t_row;
+      uint8_t* dst_row = rows + r * p.row_bytes;
+      for (int v = lane; v < vecs_per_row; v += 32) {
+        const uint64_t t = t_row + 16ull * v;
+        if (t + 16 <= p.in_valid) {
+          cp_async16(dst_row + 16 * v, src_row + 16 * v);
+        } else {
+          uint8_t tmp[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) tmp[j] = (t + j < p.in_valid) ? src[j] : 0;
-        uint4 val;
-        memcpy(&val, tmp, 16);
-        *reinterpret_cast<uint4*>(dst) = val;
+          for (int j = 0; j < 16; ++j) tmp[j] = (t + j < p.in_valid) ? src_row[16 * v + j] : 0;
+          uint4 val;
+          memcpy(&val, tmp, 16);
+          *reinterpret_cast<uint4*>(dst_row + 16 * v) = val;
+        }
       }
     }
     const int vecs_per_rec = p.record_words / 4;

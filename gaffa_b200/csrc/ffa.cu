@@ -241,9 +241,7 @@ struct PassDev {
 constexpr int kWarps = kThreads / 32;
 
 // Dynamic shared memory of the search kernel: two ColBlock headers, the
-// staged schedule, then two row buffers.  The row buffers start at least
-// max_bins floats in, so a row pointer minus bins stays inside the block's
-// allocation.
+// staged schedule, then two row buffers.
 extern __shared__ __align__(16) float g_smem[];
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
@@ -262,8 +260,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // One level: out row q (q < nrows) from `prev` by meta[q].  A warp per row,
 // lane j handles bins j, j+32, ...; only the last iteration can be partial.
-// The tail row is read at (j + roll) mod bins: a lane reads from t1 = tail +
-// roll + j until its index passes bins, then from t2 = t1 - bins.
+// The tail row is read at k = (j + roll) mod bins, computed branch-free as
+// min(k, k - bins) in unsigned arithmetic (k < 2 bins).
 template <int NB>
 __device__ __forceinline__ void merge_level(const MetaEntry* meta, uint32_t nrows, const float* prev, float* out,
                                             uint32_t pitch, uint32_t bins) {
@@ -276,15 +274,14 @@ __device__ __forceinline__ void merge_level(const MetaEntry* meta, uint32_t nrow
     if (m.op == kMerge) {
       uint32_t r = m.roll;
       if (r >= bins) r %= bins;
-      const uint32_t base = lane + r;
-      const int iw = (static_cast<int>(bins) - static_cast<int>(base) + 31) >> 5;  // unwrapped iterations
-      const float* t1 = prev + m.b * pitch + base;
-      const float* t2 = t1 - bins;
+      const uint32_t k0 = lane + r;       // < 2 bins
+      const uint32_t k1 = k0 - bins;      // wraps when k0 < bins
+      const float* t = prev + m.b * pitch;
 #pragma unroll
       for (int i = 0; i < NB; ++i) {
         if (i < NB - 1 || last_ok) {
-          const float* t = i < iw ? t1 : t2;
-          o[32 * i] = __fadd_rn(h[32 * i], t[32 * i]);
+          const uint32_t k = umin32(k0 + 32u * i, k1 + 32u * i);
+          o[32 * i] = __fadd_rn(h[32 * i], t[k]);
         }
       }
     } else {

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <numeric>
 #include <vector>
 
 #include "common.cuh"
@@ -299,5 +300,178 @@ extern "C" int gf_select_candidates(const gf_peak* peaks, uint64_t n, double tob
     if (o->max_candidates != 0 && cands.size() > o->max_candidates) cands.resize(o->max_candidates);
     *ncand = cands.size();
     if (out && capacity) std::memcpy(out, cands.data(), std::min<uint64_t>(capacity, cands.size()) * sizeof(gf_candidate));
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Harmonic flagging (src/gaffa/harmonic.cpp:14-311)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct HarmonicRatio {
+  int32_t num, den;
+  double value;
+};
+
+// Reduced ratios n/d (n <= max_harmonic, d <= denominator_max, n != d) by
+// value, then numerator, then denominator; duplicates removed
+// (harmonic.cpp:94-135).
+std::vector<HarmonicRatio> harmonic_ratios(uint64_t max_harmonic, uint64_t denominator_max) {
+  std::vector<HarmonicRatio> r;
+  r.reserve(max_harmonic * denominator_max);
+  for (uint64_t a = 1; a <= max_harmonic; ++a) {
+    for (uint64_t b = 1; b <= denominator_max; ++b) {
+      const uint64_t g = std::gcd(a, b);
+      if (a / g == b / g) continue;
+      r.push_back(HarmonicRatio{static_cast<int32_t>(a / g), static_cast<int32_t>(b / g),
+                                static_cast<double>(a / g) / static_cast<double>(b / g)});
+    }
+  }
+  std::sort(r.begin(), r.end(), [](const HarmonicRatio& x, const HarmonicRatio& y) {
+    if (x.value != y.value) return x.value < y.value;
+    if (x.num != y.num) return x.num < y.num;
+    return x.den < y.den;
+  });
+  r.erase(std::unique(r.begin(), r.end(),
+                      [](const HarmonicRatio& x, const HarmonicRatio& y) { return x.num == y.num && x.den == y.den; }),
+          r.end());
+  return r;
+}
+
+// The ratio nearest to x: the first with value >= x unless its predecessor
+// is strictly closer (harmonic.cpp:137-163).
+const HarmonicRatio* nearest_ratio(double x, const std::vector<HarmonicRatio>& r) {
+  if (!(x > 0.0) || r.empty()) return nullptr;
+  const auto lo = std::lower_bound(r.begin(), r.end(), x,
+                                   [](const HarmonicRatio& e, double v) { return e.value < v; });
+  const HarmonicRatio* best = lo != r.end() ? &*lo : nullptr;
+  if (lo != r.begin()) {
+    const HarmonicRatio* prev = &*(lo - 1);
+    if (best == nullptr || std::abs(prev->value - x) < std::abs(best->value - x)) best = prev;
+  }
+  return best;
+}
+
+// harmonic.cpp:21-35
+bool harmonic_rank(const gf_candidate& l, const gf_candidate& r) {
+  if (l.snr != r.snr) return l.snr > r.snr;
+  if (l.peak_count != r.peak_count) return l.peak_count > r.peak_count;
+  if (l.frequency != r.frequency) return l.frequency < r.frequency;
+  return l.dm_index < r.dm_index;
+}
+
+gf_harmonic_options default_harmonic_options() {
+  gf_harmonic_options o{};
+  o.max_harmonic = 16;
+  o.denominator_max = 5;
+  o.frequency_tolerance_bins = 1.5;
+  o.phase_distance_max = 1.0;
+  o.dm_distance_max = 3.0;
+  o.use_snr_consistency = 0;
+  o.snr_distance_max = 3.0;
+  return o;
+}
+
+}  // namespace
+
+extern "C" int gf_flag_harmonics(const gf_candidate* candidates, uint64_t n, const gf_harmonic_context* ctx,
+                                 const gf_harmonic_options* options, gf_candidate* sorted_out,
+                                 gf_harmonic_relation* rel) {
+  return guarded([&] {
+    check_arg(ctx != nullptr, "null argument");
+    const gf_harmonic_options o = options ? *options : default_harmonic_options();
+    // harmonic.cpp:37-92
+    check_arg(ctx->observation_seconds > 0.0 && std::isfinite(ctx->observation_seconds),
+              "Harmonic context observation_seconds must be finite and > 0");
+    check_arg(ctx->frequency_low_mhz > 0.0 && ctx->frequency_high_mhz > 0.0 && std::isfinite(ctx->frequency_low_mhz) &&
+                  std::isfinite(ctx->frequency_high_mhz),
+              "Harmonic context frequencies must be finite and > 0 MHz");
+    check_arg(o.max_harmonic >= 2, "Harmonic max_harmonic must be >= 2");
+    check_arg(o.denominator_max > 0, "Harmonic denominator_max must be > 0");
+    check_arg(o.frequency_tolerance_bins >= 0.0 && std::isfinite(o.frequency_tolerance_bins),
+              "Harmonic frequency_tolerance_bins must be finite and >= 0");
+    check_arg(o.phase_distance_max >= 0.0 && std::isfinite(o.phase_distance_max),
+              "Harmonic phase_distance_max must be finite and >= 0");
+    check_arg(o.dm_distance_max >= 0.0 && std::isfinite(o.dm_distance_max),
+              "Harmonic dm_distance_max must be finite and >= 0");
+    check_arg(o.snr_distance_max >= 0.0 && std::isfinite(o.snr_distance_max),
+              "Harmonic snr_distance_max must be finite and >= 0");
+    if (n == 0) return;
+    check_arg(candidates && sorted_out && rel, "null argument");
+    for (uint64_t i = 0; i < n; ++i) {
+      const gf_candidate& c = candidates[i];
+      check_arg(std::isfinite(c.dm) && std::isfinite(c.period) && std::isfinite(c.frequency) &&
+                    std::isfinite(c.duty_cycle) && std::isfinite(c.snr),
+                "Harmonic candidates must contain finite scientific values");
+      check_arg(c.frequency > 0.0 && c.period > 0.0 && c.duty_cycle > 0.0 && c.snr >= 0.0f,
+                "Harmonic candidate frequency, period, duty_cycle, and snr are invalid");
+    }
+    std::vector<gf_candidate> s(candidates, candidates + n);
+    std::sort(s.begin(), s.end(), harmonic_rank);
+    std::vector<gf_harmonic_relation> rl(n);
+    for (auto& r : rl) {
+      r = gf_harmonic_relation{};
+      r.parent_index = GF_NO_HARMONIC_PARENT;
+      r.numerator = 1;
+      r.denominator = 1;
+    }
+    const std::vector<HarmonicRatio> ratios = harmonic_ratios(o.max_harmonic, o.denominator_max);
+    const double lo = std::min(ctx->frequency_low_mhz, ctx->frequency_high_mhz);
+    const double hi = std::max(ctx->frequency_low_mhz, ctx->frequency_high_mhz);
+    const double band = std::abs(1.0 / (lo * lo) - 1.0 / (hi * hi));
+    // a candidate already flagged is neither a parent nor re-tested
+    // (harmonic.cpp:271-289)
+    for (uint64_t pi = 0; pi < n; ++pi) {
+      if (rl[pi].is_harmonic) continue;
+      const gf_candidate& p = s[pi];
+      for (uint64_t ci = pi + 1; ci < n; ++ci) {
+        if (rl[ci].is_harmonic) continue;
+        const gf_candidate& c = s[ci];
+        // harmonic.cpp:186-243
+        const HarmonicRatio* hr = nearest_ratio(c.frequency / p.frequency, ratios);
+        if (hr == nullptr) continue;
+        const double ferr = std::abs(c.frequency - p.frequency * hr->value) * ctx->observation_seconds;
+        if (ferr > o.frequency_tolerance_bins) continue;
+        const double phase = ferr / (c.frequency >= p.frequency ? c.duty_cycle : p.duty_cycle);
+        if (phase > o.phase_distance_max) continue;
+        const double delay_s = std::abs(p.dm - c.dm) * 4.148808e3 * band / 1000.0;
+        const double dist = delay_s / std::min(p.period * p.duty_cycle, c.period * c.duty_cycle);
+        if (dist > o.dm_distance_max) continue;
+        const double esnr = static_cast<double>(p.snr) /
+                            std::sqrt(static_cast<double>(hr->num) * static_cast<double>(hr->den));
+        const double sdist = std::abs(static_cast<double>(c.snr) - esnr);
+        if (o.use_snr_consistency && sdist > o.snr_distance_max) continue;
+        gf_harmonic_relation& r = rl[ci];
+        r.is_harmonic = 1;
+        r.parent_index = pi;
+        r.numerator = hr->num;
+        r.denominator = hr->den;
+        r.frequency_error_bins = ferr;
+        r.phase_distance = phase;
+        r.dm_distance = dist;
+        r.expected_snr = esnr;
+        r.snr_distance = sdist;
+      }
+    }
+    std::memcpy(sorted_out, s.data(), n * sizeof(gf_candidate));
+    std::memcpy(rel, rl.data(), n * sizeof(gf_harmonic_relation));
+  });
+}
+
+extern "C" int gf_remove_harmonics(const gf_candidate* sorted, const gf_harmonic_relation* rel, uint64_t n,
+                                   uint64_t max_candidates, gf_candidate* out, uint64_t* nout) {
+  return guarded([&] {
+    check_arg(nout != nullptr, "null argument");
+    *nout = 0;
+    if (n == 0) return;
+    check_arg(sorted && rel && out, "null argument");
+    uint64_t k = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+      if (rel[i].is_harmonic) continue;
+      out[k++] = sorted[i];
+      if (max_candidates != 0 && k >= max_candidates) break;
+    }
+    *nout = k;
   });
 }

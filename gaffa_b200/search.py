@@ -1,6 +1,6 @@
 """The DM-search pipeline on one GPU: filterbank -> dedispersion -> detrend +
 normalise -> per-octave downsampling + FFA + boxcar S/N -> peaks ->
-candidates -> fold of the best candidate.
+candidates -> harmonic flagging -> fold of the best candidate.
 
 This is the chain the reference wires up in
 benchmarks/cuda_dm_search_benchmark.cpp:179-260 (plus select_candidates_cpu
@@ -30,6 +30,11 @@ class SearchResult:
     ndm: int
     timings: dict
     gpu_launches: int = 0
+    # flag_harmonics_cpu of the candidates (harmonic.cpp:245-292): ranked
+    # candidates and their relations (HARMONIC_DTYPE), then the survivors
+    ranked: np.ndarray | None = None
+    harmonics: np.ndarray | None = None
+    unique_candidates: np.ndarray | None = None
 
     @property
     def dm_trial_samples(self) -> int:
@@ -64,8 +69,12 @@ class DmSearch:
                  min_points: int = 101, snr_threshold: float = 8.0, nbits: int = 8,
                  algorithm: str = "brute", subband_channels: int = 32, ndm_per_nominal: int = 32,
                  frequency_cluster_radius: float = 0.1, dm_cluster_radius: int = 1, fold_nbin: int = 64,
-                 dm_batch: int | None = None, memory_budget: int | None = None, device_id: int = 0):
+                 dm_batch: int | None = None, memory_budget: int | None = None, device_id: int = 0,
+                 harmonic_options=None):
         self.device = torch.device("cuda", device_id)
+        freq = np.asarray(frequency_mhz, dtype=np.float64)
+        self.frequency_low_mhz, self.frequency_high_mhz = float(freq.min()), float(freq.max())
+        self.harmonic_options = harmonic_options if harmonic_options is not None else core.harmonic_options()
         self.nsamples, self.tsamp = nsamples, tsamp
         self.dm_low, self.dm_step, self.ndm = dm_low, dm_step, ndm
         self.snr_threshold = snr_threshold
@@ -161,6 +170,11 @@ class DmSearch:
         peaks = core.sort_peaks(peaks)
         tobs = self.nsamples * self.tsamp if observation_seconds is None else observation_seconds
         cands = core.select_candidates(peaks, tobs, self.frequency_cluster_radius, self.dm_cluster_radius)
+        # the step after candidate selection in the reference's drivers
+        # (cuda_dm_search_benchmark.cpp:287-292)
+        ranked, rel = core.flag_harmonics(cands, tobs, self.frequency_low_mhz, self.frequency_high_mhz,
+                                          self.harmonic_options)
+        unique = core.remove_harmonics(ranked, rel)
         t3 = time.perf_counter()
         prof = expo = None
         if len(cands):
@@ -169,7 +183,8 @@ class DmSearch:
         t4 = time.perf_counter()
         t.update(stage=t1 - t0, search=t2 - t1, candidates=t3 - t2, fold=t4 - t3, total=t4 - t0)
         return SearchResult(peaks=peaks, candidates=cands, fold_profile=prof, fold_exposure=expo, nout=self.nout,
-                            ndm=self.ndm, timings=t, gpu_launches=launches + 1)
+                            ndm=self.ndm, timings=t, gpu_launches=launches + 1, ranked=ranked, harmonics=rel,
+                            unique_candidates=unique)
 
 
 def from_config(cfg, **overrides) -> DmSearch:

@@ -346,6 +346,58 @@ int gf_select_candidates(const gf_peak* peaks, uint64_t npeaks,
                          gf_candidate* out, uint64_t capacity,
                          uint64_t* ncandidates);
 
+/* HarmonicContext, include/gaffa/harmonic.h:16-20. */
+typedef struct {
+  double observation_seconds;
+  double frequency_low_mhz;
+  double frequency_high_mhz;
+} gf_harmonic_context;
+
+/* HarmonicOptions, include/gaffa/harmonic.h:22-36 (defaults: 16, 5, 1.5,
+ * 1.0, 3.0, 0, 3.0). */
+typedef struct {
+  uint64_t max_harmonic;
+  uint64_t denominator_max;
+  double frequency_tolerance_bins;
+  double phase_distance_max;
+  double dm_distance_max;
+  int32_t use_snr_consistency;
+  int32_t reserved;
+  double snr_distance_max;
+} gf_harmonic_options;
+
+#define GF_NO_HARMONIC_PARENT UINT64_MAX
+
+/* HarmonicRelation, include/gaffa/harmonic.h:38-48. */
+typedef struct {
+  int32_t is_harmonic;
+  int32_t reserved;
+  uint64_t parent_index; /* GF_NO_HARMONIC_PARENT when not a harmonic */
+  int32_t numerator;
+  int32_t denominator;
+  double frequency_error_bins;
+  double phase_distance;
+  double dm_distance;
+  double expected_snr;
+  double snr_distance;
+} gf_harmonic_relation;
+
+/* Replaces flag_harmonics_cpu, src/gaffa/harmonic.cpp:245-292.  Writes the n
+ * candidates in harmonic ranking order (S/N desc, peak_count desc, frequency
+ * asc, dm_index asc) to sorted_out and their relations to relations_out
+ * (parent_index refers to that order).  options may be NULL (defaults). */
+int gf_flag_harmonics(const gf_candidate* candidates, uint64_t n,
+                      const gf_harmonic_context* context,
+                      const gf_harmonic_options* options,
+                      gf_candidate* sorted_out,
+                      gf_harmonic_relation* relations_out);
+
+/* Replaces remove_harmonics_cpu, src/gaffa/harmonic.cpp:294-309: the
+ * non-harmonic candidates in order, at most max_candidates (0 = all). */
+int gf_remove_harmonics(const gf_candidate* sorted, const gf_harmonic_relation* relations,
+                        uint64_t n, uint64_t max_candidates, gf_candidate* out,
+                        uint64_t* nout);
+
 /* ------------------------------------------------------------------------ */
 /* Folding                                                                   */
 /* ------------------------------------------------------------------------ */

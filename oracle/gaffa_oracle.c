@@ -1193,3 +1193,160 @@ int gfo_fold_time_series_u32(const uint32_t* in, uint64_t n, double period,
   if (rc) return rc;
   FOLD_BODY((double)in[i])
 }
+
+/* ------------------------------------------------------------------------ */
+/* harmonics: harmonic.cpp:14-311                                            */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int32_t num, den;
+  double value;
+} h_ratio;
+
+static uint64_t gcd_u64(uint64_t a, uint64_t b) {
+  while (b) {
+    const uint64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+static int cmp_ratio(const void* a, const void* b) {
+  const h_ratio* l = (const h_ratio*)a;
+  const h_ratio* r = (const h_ratio*)b;
+  if (l->value != r->value) return l->value < r->value ? -1 : 1;
+  if (l->num != r->num) return l->num < r->num ? -1 : 1;
+  if (l->den != r->den) return l->den < r->den ? -1 : 1;
+  return 0;
+}
+
+/* harmonic.cpp:21-35: S/N desc, peak_count desc, frequency asc, dm_index asc */
+static int cmp_harmonic_rank(const void* a, const void* b) {
+  const gfo_candidate* l = (const gfo_candidate*)a;
+  const gfo_candidate* r = (const gfo_candidate*)b;
+  if (l->snr != r->snr) return l->snr > r->snr ? -1 : 1;
+  if (l->peak_count != r->peak_count) return l->peak_count > r->peak_count ? -1 : 1;
+  if (l->frequency != r->frequency) return l->frequency < r->frequency ? -1 : 1;
+  if (l->dm_index != r->dm_index) return l->dm_index < r->dm_index ? -1 : 1;
+  return 0;
+}
+
+/* nearest ratio to x (harmonic.cpp:137-163): the first ratio with value >= x,
+ * replaced by its predecessor only when that is strictly closer */
+static const h_ratio* nearest_ratio(double x, const h_ratio* r, uint64_t nr) {
+  if (!(x > 0.0) || nr == 0) return NULL;
+  uint64_t lo = 0, hi = nr;
+  while (lo < hi) {
+    const uint64_t mid = lo + (hi - lo) / 2;
+    if (r[mid].value < x) lo = mid + 1; else hi = mid;
+  }
+  const h_ratio* best = lo < nr ? &r[lo] : NULL;
+  if (lo > 0 && (best == NULL || fabs(r[lo - 1].value - x) < fabs(best->value - x))) best = &r[lo - 1];
+  return best;
+}
+
+int gfo_flag_harmonics(const gfo_candidate* in, uint64_t n, const gfo_harmonic_context* ctx,
+                       const gfo_harmonic_options* o, gfo_candidate* sorted,
+                       gfo_harmonic_relation* rel) {
+  /* harmonic.cpp:37-92 validation */
+  if (!(ctx->observation_seconds > 0.0) || !isfinite(ctx->observation_seconds))
+    return fail(GFO_EINVAL, "Harmonic context observation_seconds must be finite and > 0");
+  if (!(ctx->frequency_low_mhz > 0.0) || !(ctx->frequency_high_mhz > 0.0) ||
+      !isfinite(ctx->frequency_low_mhz) || !isfinite(ctx->frequency_high_mhz))
+    return fail(GFO_EINVAL, "Harmonic context frequencies must be finite and > 0 MHz");
+  if (o->max_harmonic < 2) return fail(GFO_EINVAL, "Harmonic max_harmonic must be >= 2");
+  if (o->denominator_max == 0) return fail(GFO_EINVAL, "Harmonic denominator_max must be > 0");
+  if (o->frequency_tolerance_bins < 0.0 || !isfinite(o->frequency_tolerance_bins))
+    return fail(GFO_EINVAL, "Harmonic frequency_tolerance_bins must be finite and >= 0");
+  if (o->phase_distance_max < 0.0 || !isfinite(o->phase_distance_max))
+    return fail(GFO_EINVAL, "Harmonic phase_distance_max must be finite and >= 0");
+  if (o->dm_distance_max < 0.0 || !isfinite(o->dm_distance_max))
+    return fail(GFO_EINVAL, "Harmonic dm_distance_max must be finite and >= 0");
+  if (o->snr_distance_max < 0.0 || !isfinite(o->snr_distance_max))
+    return fail(GFO_EINVAL, "Harmonic snr_distance_max must be finite and >= 0");
+  if (n == 0) return GFO_OK;
+  for (uint64_t i = 0; i < n; ++i) {
+    const gfo_candidate* c = &in[i];
+    if (!isfinite(c->dm) || !isfinite(c->period) || !isfinite(c->frequency) ||
+        !isfinite(c->duty_cycle) || !isfinite(c->snr))
+      return fail(GFO_EINVAL, "Harmonic candidates must contain finite scientific values");
+    if (!(c->frequency > 0.0) || !(c->period > 0.0) || !(c->duty_cycle > 0.0) || !(c->snr >= 0.0f))
+      return fail(GFO_EINVAL, "Harmonic candidate frequency, period, duty_cycle, and snr are invalid");
+  }
+  memcpy(sorted, in, n * sizeof(gfo_candidate));
+  qsort(sorted, n, sizeof(gfo_candidate), cmp_harmonic_rank);
+  for (uint64_t i = 0; i < n; ++i) {
+    memset(&rel[i], 0, sizeof rel[i]);
+    rel[i].parent_index = UINT64_MAX;
+    rel[i].numerator = 1;
+    rel[i].denominator = 1;
+  }
+  /* harmonic.cpp:94-135: reduced n/d with n != d, sorted, unique */
+  h_ratio* r = (h_ratio*)malloc(o->max_harmonic * o->denominator_max * sizeof(h_ratio));
+  if (!r) return fail(GFO_ENOMEM, "out of memory");
+  uint64_t nr = 0;
+  for (uint64_t a = 1; a <= o->max_harmonic; ++a)
+    for (uint64_t b = 1; b <= o->denominator_max; ++b) {
+      const uint64_t g = gcd_u64(a, b);
+      if (a / g == b / g) continue;
+      r[nr].num = (int32_t)(a / g);
+      r[nr].den = (int32_t)(b / g);
+      r[nr].value = (double)(a / g) / (double)(b / g);
+      ++nr;
+    }
+  qsort(r, nr, sizeof(h_ratio), cmp_ratio);
+  uint64_t u = 0;
+  for (uint64_t i = 0; i < nr; ++i)
+    if (u == 0 || r[i].num != r[u - 1].num || r[i].den != r[u - 1].den) r[u++] = r[i];
+  nr = u;
+  const double low = fmin(ctx->frequency_low_mhz, ctx->frequency_high_mhz);
+  const double high = fmax(ctx->frequency_low_mhz, ctx->frequency_high_mhz);
+  for (uint64_t pi = 0; pi < n; ++pi) {
+    if (rel[pi].is_harmonic) continue;
+    const gfo_candidate* p = &sorted[pi];
+    for (uint64_t ci = pi + 1; ci < n; ++ci) {
+      if (rel[ci].is_harmonic) continue;
+      const gfo_candidate* c = &sorted[ci];
+      /* harmonic.cpp:186-243 test_harmonic_relation */
+      const h_ratio* hr = nearest_ratio(c->frequency / p->frequency, r, nr);
+      if (!hr) continue;
+      const double expected = p->frequency * hr->value;
+      const double ferr = fabs(c->frequency - expected) * ctx->observation_seconds;
+      if (ferr > o->frequency_tolerance_bins) continue;
+      const double fast_duty = c->frequency >= p->frequency ? c->duty_cycle : p->duty_cycle;
+      const double phase = ferr / fast_duty;
+      if (phase > o->phase_distance_max) continue;
+      const double delay_ms = fabs(p->dm - c->dm) * 4.148808e3 * fabs(1.0 / (low * low) - 1.0 / (high * high));
+      const double wp = p->period * p->duty_cycle, wc = c->period * c->duty_cycle;
+      const double dist = (delay_ms / 1000.0) / (wp < wc ? wp : wc);
+      if (dist > o->dm_distance_max) continue;
+      const double esnr = (double)p->snr / sqrt((double)hr->num * (double)hr->den);
+      const double sdist = fabs((double)c->snr - esnr);
+      if (o->use_snr_consistency && sdist > o->snr_distance_max) continue;
+      rel[ci].is_harmonic = 1;
+      rel[ci].parent_index = pi;
+      rel[ci].numerator = hr->num;
+      rel[ci].denominator = hr->den;
+      rel[ci].frequency_error_bins = ferr;
+      rel[ci].phase_distance = phase;
+      rel[ci].dm_distance = dist;
+      rel[ci].expected_snr = esnr;
+      rel[ci].snr_distance = sdist;
+    }
+  }
+  free(r);
+  return GFO_OK;
+}
+
+int gfo_remove_harmonics(const gfo_candidate* sorted, const gfo_harmonic_relation* rel, uint64_t n,
+                         uint64_t max_candidates, gfo_candidate* out, uint64_t* nout) {
+  uint64_t k = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (rel[i].is_harmonic) continue;
+    out[k++] = sorted[i];
+    if (max_candidates != 0 && k >= max_candidates) break;
+  }
+  *nout = k;
+  return GFO_OK;
+}

@@ -191,6 +191,48 @@ int gfo_select_candidates(const gfo_peak* peaks, uint64_t npeaks,
                           const gfo_candidate_options* options,
                           gfo_candidate** candidates, uint64_t* ncandidates);
 
+/* ---- harmonics (harmonic.cpp) ---- */
+typedef struct {
+  double observation_seconds;
+  double frequency_low_mhz;
+  double frequency_high_mhz;
+} gfo_harmonic_context; /* harmonic.h:16-20 HarmonicContext */
+
+typedef struct {
+  uint64_t max_harmonic;
+  uint64_t denominator_max;
+  double frequency_tolerance_bins;
+  double phase_distance_max;
+  double dm_distance_max;
+  int32_t use_snr_consistency;
+  int32_t reserved;
+  double snr_distance_max;
+} gfo_harmonic_options; /* harmonic.h:22-36 HarmonicOptions */
+
+typedef struct {
+  int32_t is_harmonic;
+  int32_t reserved;
+  uint64_t parent_index;
+  int32_t numerator;
+  int32_t denominator;
+  double frequency_error_bins;
+  double phase_distance;
+  double dm_distance;
+  double expected_snr;
+  double snr_distance;
+} gfo_harmonic_relation; /* harmonic.h:38-48 HarmonicRelation */
+
+/* flag_harmonics_cpu (harmonic.cpp:245-292): candidates in harmonic ranking
+ * order into sorted_out, their relations into relations_out. */
+int gfo_flag_harmonics(const gfo_candidate* candidates, uint64_t n,
+                       const gfo_harmonic_context* context,
+                       const gfo_harmonic_options* options,
+                       gfo_candidate* sorted_out, gfo_harmonic_relation* relations_out);
+/* remove_harmonics_cpu (harmonic.cpp:294-309) */
+int gfo_remove_harmonics(const gfo_candidate* sorted, const gfo_harmonic_relation* relations,
+                         uint64_t n, uint64_t max_candidates, gfo_candidate* out,
+                         uint64_t* nout);
+
 /* ---- folding (folding.cpp) ---- */
 int gfo_fold_time_series_f32(const float* in, uint64_t n, double period,
                              double tsamp, uint64_t nbin, uint64_t start_sample,

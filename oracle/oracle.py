@@ -52,6 +52,24 @@ class PreprocessOptions(C.Structure):
                 ("normalise", C.c_int32), ("reject_constant", C.c_int32)]
 
 
+HARMONIC_DTYPE = np.dtype([
+    ("is_harmonic", "<i4"), ("reserved", "<i4"), ("parent_index", "<u8"), ("numerator", "<i4"),
+    ("denominator", "<i4"), ("frequency_error_bins", "<f8"), ("phase_distance", "<f8"),
+    ("dm_distance", "<f8"), ("expected_snr", "<f8"), ("snr_distance", "<f8")])
+
+
+class HarmonicContext(C.Structure):
+    _fields_ = [("observation_seconds", C.c_double), ("frequency_low_mhz", C.c_double),
+                ("frequency_high_mhz", C.c_double)]
+
+
+class HarmonicOptions(C.Structure):
+    _fields_ = [("max_harmonic", C.c_uint64), ("denominator_max", C.c_uint64),
+                ("frequency_tolerance_bins", C.c_double), ("phase_distance_max", C.c_double),
+                ("dm_distance_max", C.c_double), ("use_snr_consistency", C.c_int32),
+                ("reserved", C.c_int32), ("snr_distance_max", C.c_double)]
+
+
 class CandidateOptions(C.Structure):
     _fields_ = [("frequency_cluster_radius", C.c_double),
                 ("dm_cluster_radius", C.c_uint64),
@@ -260,6 +278,31 @@ class Oracle:
             peaks.ctypes.data_as(C.c_void_p), C.c_uint64(len(peaks)),
             C.c_double(observation_seconds), C.byref(o), C.byref(cp), C.byref(n)))
         return self._take(cp, n.value, CAND_DTYPE)
+
+    def flag_harmonics(self, candidates, observation_seconds, frequency_low_mhz, frequency_high_mhz,
+                       max_harmonic=16, denominator_max=5, frequency_tolerance_bins=1.5,
+                       phase_distance_max=1.0, dm_distance_max=3.0, use_snr_consistency=False,
+                       snr_distance_max=3.0):
+        candidates = np.ascontiguousarray(candidates, CAND_DTYPE)
+        ctx = HarmonicContext(observation_seconds, frequency_low_mhz, frequency_high_mhz)
+        o = HarmonicOptions(max_harmonic, denominator_max, frequency_tolerance_bins, phase_distance_max,
+                            dm_distance_max, int(use_snr_consistency), 0, snr_distance_max)
+        out = np.zeros(len(candidates), CAND_DTYPE)
+        rel = np.zeros(len(candidates), HARMONIC_DTYPE)
+        self._check(self._fn("flag_harmonics")(
+            candidates.ctypes.data_as(C.c_void_p), C.c_uint64(len(candidates)), C.byref(ctx), C.byref(o),
+            out.ctypes.data_as(C.c_void_p), rel.ctypes.data_as(C.c_void_p)))
+        return out, rel
+
+    def remove_harmonics(self, sorted_candidates, relations, max_candidates=0):
+        sorted_candidates = np.ascontiguousarray(sorted_candidates, CAND_DTYPE)
+        relations = np.ascontiguousarray(relations, HARMONIC_DTYPE)
+        out = np.zeros(len(sorted_candidates), CAND_DTYPE)
+        n = C.c_uint64()
+        self._check(self._fn("remove_harmonics")(
+            sorted_candidates.ctypes.data_as(C.c_void_p), relations.ctypes.data_as(C.c_void_p),
+            C.c_uint64(len(out)), C.c_uint64(max_candidates), out.ctypes.data_as(C.c_void_p), C.byref(n)))
+        return out[: n.value]
 
     def fold(self, x, period, tsamp, nbin, start_sample=0):
         x = np.ascontiguousarray(x)

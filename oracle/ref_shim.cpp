@@ -16,6 +16,7 @@
 #include "gaffa/ffa_plan.h"
 #include "gaffa/ffa_search.h"
 #include "gaffa/folding.h"
+#include "gaffa/harmonic.h"
 #include "gaffa/preprocessing.h"
 #include "gaffa/time_series.h"
 
@@ -389,6 +390,91 @@ int gfr_fold_time_series_u32(const uint32_t* in, uint64_t n, double period,
                            .start_sample = start});
     std::memcpy(profile, r.profile.data(), nbin * sizeof(float));
     std::memcpy(exposure, r.exposure.data(), nbin * sizeof(double));
+  });
+}
+
+
+int gfr_flag_harmonics(const gfo_candidate* in, uint64_t n, const gfo_harmonic_context* ctx,
+                       const gfo_harmonic_options* o, gfo_candidate* sorted,
+                       gfo_harmonic_relation* rel) {
+  return guarded([&] {
+    std::vector<gaffa::Candidate> cands;
+    for (uint64_t i = 0; i < n; ++i) {
+      const gfo_candidate& c = in[i];
+      gaffa::Candidate x{};
+      x.dm = c.dm;
+      x.dm_index = c.dm_index;
+      x.period = c.period;
+      x.frequency = c.frequency;
+      x.width = c.width;
+      x.duty_cycle = c.duty_cycle;
+      x.snr = c.snr;
+      x.peak_count = c.peak_count;
+      x.dm_index_min = c.dm_index_min;
+      x.dm_index_max = c.dm_index_max;
+      x.frequency_min = c.frequency_min;
+      x.frequency_max = c.frequency_max;
+      x.best_peak = from_peak(c.best_peak);
+      cands.push_back(x);
+    }
+    const auto r = gaffa::flag_harmonics_cpu(
+        cands,
+        gaffa::HarmonicContext{.observation_seconds = ctx->observation_seconds,
+                               .frequency_low_mhz = ctx->frequency_low_mhz,
+                               .frequency_high_mhz = ctx->frequency_high_mhz},
+        gaffa::HarmonicOptions{.max_harmonic = o->max_harmonic,
+                               .denominator_max = o->denominator_max,
+                               .frequency_tolerance_bins = o->frequency_tolerance_bins,
+                               .phase_distance_max = o->phase_distance_max,
+                               .dm_distance_max = o->dm_distance_max,
+                               .use_snr_consistency = o->use_snr_consistency != 0,
+                               .snr_distance_max = o->snr_distance_max});
+    for (size_t i = 0; i < r.size(); ++i) {
+      const gaffa::Candidate& c = r[i].candidate;
+      gfo_candidate& x = sorted[i];
+      std::memset(&x, 0, sizeof x);
+      x.dm = c.dm;
+      x.dm_index = c.dm_index;
+      x.period = c.period;
+      x.frequency = c.frequency;
+      x.width = c.width;
+      x.duty_cycle = c.duty_cycle;
+      x.snr = c.snr;
+      x.peak_count = c.peak_count;
+      x.dm_index_min = c.dm_index_min;
+      x.dm_index_max = c.dm_index_max;
+      x.frequency_min = c.frequency_min;
+      x.frequency_max = c.frequency_max;
+      x.best_peak = to_peak(c.best_peak.peak, c.best_peak.dm, c.best_peak.dm_index);
+      const gaffa::HarmonicRelation& h = r[i].harmonic;
+      gfo_harmonic_relation& y = rel[i];
+      std::memset(&y, 0, sizeof y);
+      y.is_harmonic = h.is_harmonic ? 1 : 0;
+      y.parent_index = h.parent_index;
+      y.numerator = h.numerator;
+      y.denominator = h.denominator;
+      y.frequency_error_bins = h.frequency_error_bins;
+      y.phase_distance = h.phase_distance;
+      y.dm_distance = h.dm_distance;
+      y.expected_snr = h.expected_snr;
+      y.snr_distance = h.snr_distance;
+    }
+  });
+}
+
+int gfr_remove_harmonics(const gfo_candidate* sorted, const gfo_harmonic_relation* rel, uint64_t n,
+                         uint64_t max_candidates, gfo_candidate* out, uint64_t* nout) {
+  return guarded([&] {
+    // round-trip through the reference types: only is_harmonic and the
+    // candidate order matter to remove_harmonics_cpu
+    std::vector<gaffa::HarmonicCandidate> in(n);
+    for (uint64_t i = 0; i < n; ++i) {
+      in[i].candidate.frequency = static_cast<double>(i);  // index carrier
+      in[i].harmonic.is_harmonic = rel[i].is_harmonic != 0;
+    }
+    const auto r = gaffa::remove_harmonics_cpu(in, max_candidates);
+    for (size_t i = 0; i < r.size(); ++i) out[i] = sorted[static_cast<uint64_t>(r[i].frequency)];
+    *nout = r.size();
   });
 }
 

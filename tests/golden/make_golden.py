@@ -9,6 +9,7 @@ from the reference's own functions through ``oracle/ref_shim.cpp``:
 
 Writes
   ref_small.npz            small seeded cases for every hot-path function
+  ref_harmonic.npz         seeded candidate lists through flag_harmonics_cpu
   ref_plain_end_to_end.npz the full plain end-to-end workload (256 ch, 2^18
                            samples, 512 DMs): digests of the dedispersed block
                            and of all raw peaks, the candidate list and the
@@ -171,12 +172,77 @@ def plain_end_to_end(ref: Oracle) -> dict:
     }
 
 
+def harmonic_candidates(rng: np.random.Generator, n: int) -> np.ndarray:
+    """Candidate lists with harmonic families: parents at random frequencies,
+    children at n/d multiples (small frequency jitter), nearby DMs, and
+    unrelated candidates."""
+    from oracle.oracle import CAND_DTYPE
+    c = np.zeros(n, CAND_DTYPE)
+    nparent = max(1, n // 4)
+    pf = rng.uniform(0.1, 10.0, nparent)
+    pdm = rng.uniform(0.0, 500.0, nparent)
+    for i in range(n):
+        if i < nparent:
+            f, dm = pf[i], pdm[i]
+        elif rng.random() < 0.7:
+            j = rng.integers(nparent)
+            num, den = rng.integers(1, 9), rng.integers(1, 6)
+            f = pf[j] * num / den * (1.0 + rng.normal(0, 2e-4))
+            dm = pdm[j] + rng.normal(0, 2.0)
+        else:
+            f, dm = rng.uniform(0.1, 10.0), rng.uniform(0.0, 500.0)
+        duty = rng.choice([0.01, 0.02, 0.05, 0.1])
+        c[i]["frequency"] = f
+        c[i]["period"] = 1.0 / f
+        c[i]["dm"] = max(dm, 0.0)
+        c[i]["dm_index"] = int(max(dm, 0.0) * 2)
+        c[i]["duty_cycle"] = duty
+        c[i]["width"] = max(1, int(round(duty * 200)))
+        c[i]["snr"] = np.float32(rng.uniform(6.0, 40.0))
+        c[i]["peak_count"] = rng.integers(1, 50)
+        c[i]["dm_index_min"] = c[i]["dm_index"]
+        c[i]["dm_index_max"] = c[i]["dm_index"]
+        c[i]["frequency_min"] = f
+        c[i]["frequency_max"] = f
+    return c
+
+
+def harmonic_cases(ref: Oracle) -> dict:
+    out = {}
+    rng = np.random.default_rng(4321)
+    options = [dict(), dict(max_harmonic=8, denominator_max=3), dict(frequency_tolerance_bins=3.0,
+               phase_distance_max=2.0, dm_distance_max=10.0), dict(use_snr_consistency=True, snr_distance_max=5.0)]
+    for k, opts in enumerate(options):
+        cands = harmonic_candidates(rng, 60 + 20 * k)
+        ctx = (rng.uniform(50.0, 600.0), 1100.0, 1700.0)
+        srt, rel = ref.flag_harmonics(cands, *ctx, **opts)
+        out[f"h{k}_in"] = cands
+        out[f"h{k}_ctx"] = np.array(ctx)
+        out[f"h{k}_sorted"] = srt
+        out[f"h{k}_rel"] = rel
+        out[f"h{k}_kept"] = ref.remove_harmonics(srt, rel, 10)
+    # the plain end-to-end candidate list, as the pipeline flags it
+    plain = OUT / "ref_plain_end_to_end.npz"
+    if plain.exists():
+        cfg = configs.plain_end_to_end()
+        f = cfg.obs.frequencies
+        ctx = (cfg.obs.nsamples * cfg.obs.tsamp, float(f.min()), float(f.max()))
+        srt, rel = ref.flag_harmonics(np.load(plain)["candidates"], *ctx)
+        out["plain_ctx"] = np.array(ctx)
+        out["plain_sorted"] = srt
+        out["plain_rel"] = rel
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-small", action="store_true")
     args = ap.parse_args()
     ref = Oracle("reference")
-    np.savez_compressed(OUT / "ref_small.npz", **small_cases(ref))
+    np.savez_compressed(OUT / "ref_harmonic.npz", **harmonic_cases(ref))
+    if not args.skip_small:
+        np.savez_compressed(OUT / "ref_small.npz", **small_cases(ref))
     if not args.skip_plain:
         np.savez_compressed(OUT / "ref_plain_end_to_end.npz", **plain_end_to_end(ref))
 

@@ -7,6 +7,7 @@ is compared to 1e-6 relative.  Fixtures come from the reference's CPU sources
 (tests/golden/make_golden.py); randomised cases use the C restatement.
 """
 import hashlib
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -268,6 +269,9 @@ def test_plain_end_to_end_matches_reference(golden_plain):
     assert hashlib.sha256(res.peaks.tobytes()).hexdigest() == str(g["peaks_digest"])
     assert np.array_equal(res.candidates, g["candidates"])
     np.testing.assert_allclose(res.fold_profile, g["fold_profile"], rtol=FOLD_RTOL)
+    h = np.load(Path(__file__).resolve().parent / "golden" / "ref_harmonic.npz")
+    assert np.array_equal(res.ranked, h["plain_sorted"])
+    assert np.array_equal(res.harmonics, h["plain_rel"])
 
 
 def test_invalid_arguments_raise_before_launch():
