@@ -88,6 +88,20 @@ class HarmonicOptions(C.Structure):
                 ("reserved", i32), ("snr_distance_max", dbl)]
 
 
+class FilterbankHeader(C.Structure):
+    _fields_ = [("header_size", C.c_int64), ("nsamples", C.c_int64)] + \
+        [(n, i32) for n in ("telescope_id", "machine_id", "data_type", "barycentric", "pulsarcentric", "ibeam",
+                            "nbeams", "npuls", "nbins", "nbits", "nifs", "nchans")] + \
+        [(n, dbl) for n in ("az_start", "za_start", "src_raj", "src_dej", "tstart", "tsamp", "fch1", "foff",
+                            "refdm", "period")] + \
+        [("uses_frequency_table", i32), ("reversed", i32), ("rawdatafile", C.c_char * 256),
+         ("source_name", C.c_char * 256)]
+
+
+CHANNEL_ORDER_ASCENDING = 0
+CHANNEL_ORDER_FILE = 1
+
+
 class SynthPulsar(C.Structure):
     _fields_ = [("period", dbl), ("dm", dbl), ("duty_cycle", dbl), ("amplitude", dbl), ("phase", dbl)]
 
@@ -158,6 +172,11 @@ _SIGNATURES = [
     ("gf_synth_generate", C.c_int, [C.POINTER(SynthDesc), u64, u64, vp, vp]),
     ("gf_fold_noalloc_max_bytes", u64, []),
     ("gf_fold_time_series_noalloc", C.c_int, [vp, i32, u64, dbl, dbl, u64, u64, vp, vp, vp, vp]),
+    ("gf_dedisperse_spectrum", C.c_int, [vp, i32, u64, u64, C.POINTER(dbl), dbl, dbl, dbl, u64, u64, vp,
+                                         C.POINTER(u64), vp]),
+    ("gf_filterbank_read_header", C.c_int, [C.c_char_p, i32, C.POINTER(FilterbankHeader), vp, u64]),
+    ("gf_filterbank_read_host", C.c_int, [C.c_char_p, i32, u64, u64, vp]),
+    ("gf_filterbank_load", C.c_int, [C.c_char_p, i32, u64, u64, vp, vp, u64, vp]),
     ("gf_flag_harmonics", C.c_int, [vp, u64, C.POINTER(HarmonicContext), C.POINTER(HarmonicOptions), vp, vp]),
     ("gf_remove_harmonics", C.c_int, [vp, vp, u64, u64, vp, C.POINTER(u64)]),
 ]

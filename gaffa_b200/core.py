@@ -371,6 +371,97 @@ def select_candidates(peaks: np.ndarray, observation_seconds: float, frequency_c
     return out
 
 
+def dedisperse_spectrum(filterbank: torch.Tensor, frequency_mhz, dm: float, tsamp: float,
+                        ref_frequency_mhz: float | None = None, chan_begin: int = 0, chan_end: int | None = None,
+                        stream=None) -> torch.Tensor:
+    """dedisperse_spectrum_cpu / _cuda (src/gaffa/dedispersion.cpp:249-289) on a
+    device-resident time-major [nsamples][nchans] filterbank (uint8, int16
+    holding uint16, or float32): [nout][chan_end - chan_begin], each channel
+    shifted by its delay at dm."""
+    if filterbank.dim() != 2 or not filterbank.is_cuda:
+        raise ValueError("filterbank must be a 2-D CUDA tensor [nsamples][nchans]")
+    elem = {torch.uint8: 1, torch.int16: 2, torch.uint16: 2, torch.float32: 4}.get(filterbank.dtype)
+    if elem is None:
+        raise TypeError("filterbank dtype must be uint8, uint16 or float32")
+    fb = filterbank.contiguous()
+    freq = np.ascontiguousarray(frequency_mhz, dtype=np.float64)
+    nsamples, nchans = fb.shape
+    ref = float(freq.max()) if ref_frequency_mhz is None else ref_frequency_mhz
+    ce = nchans if chan_end is None else chan_end
+    nout = _lib.u64()
+    fptr = freq.ctypes.data_as(C.POINTER(C.c_double))
+    check(_lib.lib().gf_dedisperse_spectrum(None, elem, nsamples, nchans, fptr, dm, ref, tsamp, chan_begin, ce,
+                                            None, C.byref(nout), None))
+    out = torch.empty((nout.value, ce - chan_begin), dtype=fb.dtype, device=fb.device)
+    s = stream if stream is not None else torch.cuda.current_stream(fb.device)
+    check(_lib.lib().gf_dedisperse_spectrum(ptr(fb), elem, nsamples, nchans, fptr, dm, ref, tsamp, chan_begin, ce,
+                                            ptr(out), C.byref(nout), C.c_void_p(s.cuda_stream)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# filterbank ingest
+# ---------------------------------------------------------------------------
+
+_FB_DTYPE = {8: np.uint8, 16: np.uint16, 32: np.float32}
+
+
+def read_filterbank_header(path, preserve_file_order: bool = False) -> tuple[dict, np.ndarray]:
+    """read_filterbank's header (src/gaffa/io/filterbank.cpp:116-224, 335-348):
+    the normalised fields and the delivered channels' frequencies."""
+    h = _lib.FilterbankHeader()
+    order = _lib.CHANNEL_ORDER_FILE if preserve_file_order else _lib.CHANNEL_ORDER_ASCENDING
+    p = str(path).encode()
+    check(_lib.lib().gf_filterbank_read_header(p, order, C.byref(h), None, 0))
+    freq = np.zeros(h.nchans, np.float64)
+    check(_lib.lib().gf_filterbank_read_header(p, order, C.byref(h), ptr(freq), len(freq)))
+    fields = {k: getattr(h, k) for k, _ in h._fields_}
+    fields["rawdatafile"] = h.rawdatafile.decode()
+    fields["source_name"] = h.source_name.decode()
+    return fields, freq
+
+
+def _fb_shape(h: dict, nrows: int) -> tuple[tuple, object]:
+    nbits = h["nbits"]
+    if nbits in _FB_DTYPE:
+        return (nrows, h["nifs"], h["nchans"]), _FB_DTYPE[nbits]
+    return (nrows, h["nifs"], h["nchans"] * nbits // 8), np.uint8  # packed rows
+
+
+def read_filterbank(path, preserve_file_order: bool = False, row_begin: int = 0, nrows: int | None = None):
+    """read_filterbank into host memory: (header, frequencies, samples
+    [nrows][nifs][nchans] (packed bytes for nbits < 8))."""
+    h, freq = read_filterbank_header(path, preserve_file_order)
+    n = h["nsamples"] - row_begin if nrows is None else nrows
+    shape, dt = _fb_shape(h, n)
+    out = np.zeros(shape, dt)
+    order = _lib.CHANNEL_ORDER_FILE if preserve_file_order else _lib.CHANNEL_ORDER_ASCENDING
+    check(_lib.lib().gf_filterbank_read_host(str(path).encode(), order, row_begin, n, ptr(out) if out.size else None))
+    return h, freq, out
+
+
+def load_filterbank(path, preserve_file_order: bool = False, row_begin: int = 0, nrows: int | None = None,
+                    device_id: int = 0, bounce_bytes: int = 64 << 20, stream=None):
+    """The same samples loaded straight into device memory: file reads through
+    a pinned bounce buffer overlap the host-to-device copies, and the channel
+    reversal runs on the GPU.  Returns (header, frequencies, device tensor)."""
+    h, freq = read_filterbank_header(path, preserve_file_order)
+    n = h["nsamples"] - row_begin if nrows is None else nrows
+    shape, dt = _fb_shape(h, n)
+    tdt = {np.uint8: torch.uint8, np.uint16: torch.int16, np.float32: torch.float32}[dt]
+    dev = torch.device("cuda", device_id)
+    out = torch.empty(shape, dtype=tdt, device=dev)
+    bounce = torch.empty(max(bounce_bytes, 2 * int(np.prod(shape[1:])) * np.dtype(dt).itemsize), dtype=torch.uint8,
+                         pin_memory=True)
+    order = _lib.CHANNEL_ORDER_FILE if preserve_file_order else _lib.CHANNEL_ORDER_ASCENDING
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    with torch.cuda.device(dev):
+        check(_lib.lib().gf_filterbank_load(str(path).encode(), order, row_begin, n, ptr(out) if out.numel() else None,
+                                            ptr(bounce), bounce.numel(), C.c_void_p(s.cuda_stream)))
+    s.synchronize()  # the bounce buffer is released on return
+    return h, freq, out
+
+
 def harmonic_options(max_harmonic: int = 16, denominator_max: int = 5, frequency_tolerance_bins: float = 1.5,
                      phase_distance_max: float = 1.0, dm_distance_max: float = 3.0,
                      use_snr_consistency: bool = False, snr_distance_max: float = 3.0):

@@ -70,6 +70,7 @@ struct BytesParams {
   uint64_t rec_group_stride;
   uint64_t rec_dm_stride;
   int nblocks;               // DM blocks per group in the launch (fastest grid index)
+  uint32_t one;              // 1, opaque to the compiler: accumulation through IMAD
   int dm_count;              // DMs per group handled by the launch
   int dm_count_last;         // DMs of the launch's last group
   int ngroups;
@@ -126,7 +127,7 @@ template <int S>
 __device__ __forceinline__ void accumulate_class(const uint32_t* __restrict__ smem_words,
                                                  const uint32_t* __restrict__ rec, int& pos,
                                                  int npairs, int lane_word,
-                                                 uint32_t (&e)[kWords], uint32_t (&o)[kWords]) {
+                                                 uint32_t (&e)[kWords], uint32_t (&o)[kWords], uint32_t one) {
   for (int i = 0; i < npairs; ++i) {
     const uint32_t entry = rec[pos + i];
     const uint32_t* a = smem_words + (entry & 0xffffu) + lane_word;
@@ -135,8 +136,10 @@ __device__ __forceinline__ void accumulate_class(const uint32_t* __restrict__ sm
     for (int m = 0; m < kWords; ++m) {
       const uint32_t w1 = a[32 * m];
       const uint32_t w2 = b[32 * m];
-      e[m] += (w1 & 0x00ff00ffu) + (w2 & 0x00ff00ffu);
-      o[m] += __byte_perm(w1, 0u, 0x4341) + __byte_perm(w2, 0u, 0x4341);
+      e[m] = (w1 & 0x00ff00ffu) * one + e[m];
+      e[m] = (w2 & 0x00ff00ffu) * one + e[m];
+      o[m] = __byte_perm(w1, 0u, 0x4341) * one + o[m];
+      o[m] = __byte_perm(w2, 0u, 0x4341) * one + o[m];
     }
   }
   pos += npairs;
@@ -247,10 +250,10 @@ __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesPara
       const uint32_t* rec = reinterpret_cast<const uint32_t*>(rows + rows_bytes) + dm_sub * p.record_words;
       const uint32_t counts = rec[0];
       int pos = 1;
-      accumulate_class<0>(smem_words, rec, pos, (counts & 0xffu) >> 1, lane_word, e[0], o[0]);
-      accumulate_class<1>(smem_words, rec, pos, ((counts >> 8) & 0xffu) >> 1, lane_word, e[1], o[1]);
-      accumulate_class<2>(smem_words, rec, pos, ((counts >> 16) & 0xffu) >> 1, lane_word, e[2], o[2]);
-      accumulate_class<3>(smem_words, rec, pos, (counts >> 24) >> 1, lane_word, e[3], o[3]);
+      accumulate_class<0>(smem_words, rec, pos, (counts & 0xffu) >> 1, lane_word, e[0], o[0], p.one);
+      accumulate_class<1>(smem_words, rec, pos, ((counts >> 8) & 0xffu) >> 1, lane_word, e[1], o[1], p.one);
+      accumulate_class<2>(smem_words, rec, pos, ((counts >> 16) & 0xffu) >> 1, lane_word, e[2], o[2], p.one);
+      accumulate_class<3>(smem_words, rec, pos, (counts >> 24) >> 1, lane_word, e[3], o[3], p.one);
       if ((k + 1) % chunks_per_flush == 0 || k + 1 == p.nchunks) {
         flush_class<0>(e[0], o[0], acc, lane);
         flush_class<1>(e[1], o[1], acc, lane);
@@ -302,6 +305,26 @@ __global__ void __launch_bounds__(256) subband_stage2_u32_kernel(
     if (st < inter_valid) sum += __ldg(base + b * inter_row_stride + st);
   }
   out[(static_cast<uint64_t>(group) * ndm_group + dm_local) * out_row_stride + t] = sum;
+}
+
+// Aligned single-DM spectrum: out[t][c] = in[t + d(c)][chan_begin + c].  A
+// warp per output time step, lanes over channels, so output rows are written
+// coalesced; neighbouring channels read nearby input rows (the delay varies
+// slowly across channels) and share L1/L2 lines.
+template <typename T>
+__global__ void __launch_bounds__(256) spectrum_kernel(const T* __restrict__ in, uint64_t nchans,
+                                                       uint64_t chan_begin, uint32_t nc,
+                                                       const int32_t* __restrict__ delay, uint64_t nout,
+                                                       T* __restrict__ out) {
+  const uint32_t c = blockIdx.y * 32 + (threadIdx.x & 31);
+  if (c >= nc) return;
+  const uint64_t d = static_cast<uint64_t>(delay[c]);
+  const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * 64;
+  for (uint32_t tt = threadIdx.x >> 5; tt < 64; tt += 8) {
+    const uint64_t t = t0 + tt;
+    if (t >= nout) break;
+    out[t * nc + c] = in[(t + d) * nchans + chan_begin + c];
+  }
 }
 
 // Time-major [nsamples][row_bytes] -> channel-major rows [chan][row_stride]
@@ -512,6 +535,7 @@ struct BytesStage {
     p.nout = nout;
     const int dmax = std::max(dm_count, dm_count_last);
     p.nblocks = static_cast<int>(ceil_div(dmax, launch.dms_per_cta));
+    p.one = 1u;
     const uint64_t ctas = ceil_div(nout, p.cta_samples) * static_cast<uint64_t>(p.nblocks);
     if (ctas >= (1ull << 31)) raise(GF_EINVAL, "dedispersion launch too large");
     dim3 grid(static_cast<unsigned>(ctas), 1u, static_cast<unsigned>(gcount));
@@ -812,5 +836,66 @@ extern "C" int gf_dedisp_workspace_bytes(const gf_dedisp_program* P, uint64_t dm
     const uint64_t dpc1 = P->stage1.launch.dms_per_cta;
     const uint64_t groups = std::min<uint64_t>(ceil_div(dm_count, P->npn) + 2 * dpc1, P->nnom + dpc1);
     *bytes = groups * P->nsb * P->inter_row_stride * (P->inter_u8 ? 1 : 4);
+  });
+}
+
+extern "C" int gf_dedisperse_spectrum(const void* dev_in, int32_t elem_bytes, uint64_t nsamples, uint64_t nchans,
+                                      const double* freq, double dm, double ref_frequency_mhz, double tsamp,
+                                      uint64_t chan_begin, uint64_t chan_end, void* dev_out, uint64_t* nout,
+                                      void* stream) {
+  return guarded([&] {
+    check_arg(freq != nullptr && nout != nullptr, "null argument");
+    check_arg(elem_bytes == 1 || elem_bytes == 2 || elem_bytes == 4, "elem_bytes must be 1, 2 or 4");
+    // dedispersion.cpp:99-110 validate_single_plan
+    gf_dedisp_desc d{};
+    d.nsamples = nsamples;
+    d.nchans = nchans;
+    d.frequency_mhz = freq;
+    d.dm_low = dm;
+    d.dm_step = 1.0;
+    d.ndm = 1;
+    d.ref_frequency_mhz = ref_frequency_mhz;
+    d.tsamp = tsamp;
+    d.chan_begin = chan_begin;
+    d.chan_end = chan_end;
+    d.nbits = 8;
+    d.algorithm = GF_DEDISP_BRUTE;
+    check_arg(std::isfinite(dm) && dm >= 0.0, "dm must be finite and non-negative");
+    validate_desc(d);
+    // internal/dedispersion_delay.h:52-62,121-128
+    const uint64_t nc = chan_end - chan_begin;
+    std::vector<int32_t> delays(nc);
+    double fmin = freq[chan_begin];
+    for (uint64_t c = chan_begin; c < chan_end; ++c) {
+      delays[c - chan_begin] = delay_bins(dm, freq[c], ref_frequency_mhz, tsamp);
+      fmin = std::min(fmin, freq[c]);
+    }
+    const int32_t max_delay = delay_bins(dm, fmin, ref_frequency_mhz, tsamp);
+    check_arg(max_delay >= 0, "dedispersion requires non-negative delays");
+    check_arg(static_cast<uint64_t>(max_delay) < nsamples, "dedispersion valid output range is empty");
+    *nout = nsamples - static_cast<uint64_t>(max_delay);
+    if (dev_out == nullptr) return;
+    check_arg(dev_in != nullptr, "null argument");
+    auto s = as_stream(stream);
+    int32_t* dd = nullptr;
+    cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&dd), nc * sizeof(int32_t), s), "cudaMallocAsync(delays)");
+    cuda_check(cudaMemcpyAsync(dd, delays.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice, s),
+               "cudaMemcpyAsync(delays)");
+    const dim3 grid(static_cast<unsigned>(ceil_div(*nout, 64)), static_cast<unsigned>(ceil_div(nc, 32)));
+    check_arg(ceil_div(*nout, 64) < (1ull << 31) && ceil_div(nc, 32) < 65536, "spectrum too large");
+    if (elem_bytes == 1)
+      spectrum_kernel<uint8_t><<<grid, 256, 0, s>>>(static_cast<const uint8_t*>(dev_in), nchans, chan_begin,
+                                                    static_cast<uint32_t>(nc), dd, *nout,
+                                                    static_cast<uint8_t*>(dev_out));
+    else if (elem_bytes == 2)
+      spectrum_kernel<uint16_t><<<grid, 256, 0, s>>>(static_cast<const uint16_t*>(dev_in), nchans, chan_begin,
+                                                     static_cast<uint32_t>(nc), dd, *nout,
+                                                     static_cast<uint16_t*>(dev_out));
+    else
+      spectrum_kernel<float><<<grid, 256, 0, s>>>(static_cast<const float*>(dev_in), nchans, chan_begin,
+                                                  static_cast<uint32_t>(nc), dd, *nout,
+                                                  static_cast<float*>(dev_out));
+    cuda_check(cudaGetLastError(), "spectrum_kernel launch");
+    cuda_check(cudaFreeAsync(dd, s), "cudaFreeAsync(delays)");
   });
 }

@@ -360,8 +360,23 @@ __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, u
     float* c = cp + threadIdx.x * cp_pitch;
     float acc = 0.0f;
     c[0] = 0.0f;
-#pragma unroll 8
-    for (uint32_t i = 0; i < bins; ++i) {
+    // loads of the next 8 samples overlap the current 8-add chain
+    float cur[8], nxt[8];
+    const uint32_t nfull = bins & ~7u;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) cur[j] = (static_cast<uint32_t>(j) < nfull) ? prof[j] : 0.0f;
+    for (uint32_t i = 0; i < nfull; i += 8) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) nxt[j] = (i + 8 + j < nfull) ? prof[i + 8 + j] : 0.0f;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        acc = __fadd_rn(acc, cur[j]);
+        c[i + j + 1] = acc;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) cur[j] = nxt[j];
+    }
+    for (uint32_t i = nfull; i < bins; ++i) {
       acc = __fadd_rn(acc, prof[i]);
       c[i + 1] = acc;
     }
@@ -385,11 +400,16 @@ __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, u
 #pragma unroll
       for (int i = 0; i < NB; ++i)
         if (i < NB - 1 || last_ok) best = fmaxf(best, __fsub_rn(cw[32 * i], base[i]));
-      const float maxv = key_float(__reduce_max_sync(0xffffffffu, float_key(best)));
-      const float snr = __fmul_rn(
-          __fsub_rn(__fmul_rn(__fadd_rn(tr.height, tr.baseline), maxv), __fmul_rn(tr.baseline, psum)),
+      // S/N is monotone in the boxcar sum, so the row passes the threshold
+      // exactly when some lane's own maximum does
+      const float lane_snr = __fmul_rn(
+          __fsub_rn(__fmul_rn(__fadd_rn(tr.height, tr.baseline), best), __fmul_rn(tr.baseline, psum)),
           a.inv_stdnoise);
-      if (snr >= a.threshold) {  // warp-uniform: maxv is the same on every lane
+      if (__any_sync(0xffffffffu, lane_snr >= a.threshold)) {
+        const float maxv = key_float(__reduce_max_sync(0xffffffffu, float_key(best)));
+        const float snr = __fmul_rn(
+            __fsub_rn(__fmul_rn(__fadd_rn(tr.height, tr.baseline), maxv), __fmul_rn(tr.baseline, psum)),
+            a.inv_stdnoise);
         uint32_t first = 0xffffffffu;
 #pragma unroll
         for (int i = NB - 1; i >= 0; --i)
@@ -480,8 +500,8 @@ __device__ float* eval_subtree(const SearchParams& p, const float* src, uint32_t
 }
 
 // Column block `hb`: stages its merge entries, loads its bottom rows from
-// `src` (scratch written by other CTAs of the cluster: L2 loads), evaluates
-// its levels.  The output rows (hb.count[0]) end in buf0.
+// `src` (scratch written by the cluster's CTAs in the previous phase),
+// evaluates its levels.  The output rows (hb.count[0]) end in buf0.
 template <int NB>
 __device__ void eval_block(const SearchParams& p, const ColBlock& hb, const float* src, uint32_t bins, float* buf0,
                            float* buf1, MetaEntry* cmeta) {
@@ -496,17 +516,18 @@ __device__ void eval_block(const SearchParams& p, const ColBlock& hb, const floa
   const uint32_t nb = hb.count[K];
   const uint32_t nruns = hb.nruns;
   const bool last_ok = lane + 32u * (NB - 1) < bins;
+  // Bottom rows: async copies, all in flight at once.  The rows were written
+  // by other CTAs of the cluster before the cluster barrier, whose acquire
+  // makes them visible to these (L1-allocating) reads.
   for (uint32_t q = warp; q < nb; q += kWarps) {
-    uint32_t j = 0;
-    while (j + 1 < nruns && hb.run_off[j + 1] <= q) ++j;
-    const float* g = src + static_cast<uint64_t>(hb.run_row[j] + (q - hb.run_off[j])) * bins + lane;
-    float v[NB];
+    uint32_t j = 0;  // run holding buffer row q (runs ascend in run_off)
 #pragma unroll
-    for (int i = 0; i < NB; ++i) v[i] = (i < NB - 1 || last_ok) ? __ldcg(g + 32 * i) : 0.0f;
+    for (uint32_t r = 1; r < 8; ++r) j += (r < nruns && hb.run_off[r] <= q) ? 1u : 0u;
+    const float* g = src + static_cast<uint64_t>(hb.run_row[j] + (q - hb.run_off[j])) * bins + lane;
     float* o = bottom + q * pitch + lane;
 #pragma unroll
     for (int i = 0; i < NB; ++i)
-      if (i < NB - 1 || last_ok) o[32 * i] = v[i];
+      if (i < NB - 1 || last_ok) cp_async4(o + 32 * i, g + 32 * i);
   }
   cp_async_wait_all();
   __syncthreads();

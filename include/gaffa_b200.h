@@ -165,6 +165,59 @@ int gf_dedisp_run(gf_dedisp_program* program, const void* dev_staged,
 int gf_dedisp_workspace_bytes(const gf_dedisp_program* program, uint64_t dm_count,
                               uint64_t* bytes);
 
+/* Aligned single-DM spectrum.  Replaces dedisperse_spectrum_cpu /
+ * dedisperse_spectrum_cuda (dedispersion.cpp:249-289,
+ * dedispersion_cuda.cu:295-318): channels [chan_begin, chan_end) of a
+ * time-major [nsamples][nchans] filterbank (elem_bytes 1 = uint8, 2 = uint16,
+ * 4 = float), each shifted by its delay at dm:
+ *   out[t][c] = in[t + d(c)][chan_begin + c],  t < nout,
+ * nout = nsamples - d(dm, lowest selected frequency).  Writes *nout; with
+ * dev_out == NULL only *nout is computed.  Runs on the current device. */
+int gf_dedisperse_spectrum(const void* dev_in, int32_t elem_bytes, uint64_t nsamples,
+                           uint64_t nchans, const double* frequency_mhz, double dm,
+                           double ref_frequency_mhz, double tsamp, uint64_t chan_begin,
+                           uint64_t chan_end, void* dev_out, uint64_t* nout, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Filterbank ingest (SIGPROC)                                               */
+/* ------------------------------------------------------------------------ */
+
+#define GF_CHANNEL_ORDER_ASCENDING 0 /* ChannelOrderPolicy::FrequencyAscending */
+#define GF_CHANNEL_ORDER_FILE 1      /* ChannelOrderPolicy::PreserveFileOrder */
+
+/* FilterbankHeader, include/gaffa/filterbank.h:33-65, after
+ * read_filterbank's metadata normalisation (src/gaffa/io/filterbank.cpp:105-118). */
+typedef struct {
+  int64_t header_size;
+  int64_t nsamples;
+  int32_t telescope_id, machine_id, data_type, barycentric, pulsarcentric;
+  int32_t ibeam, nbeams, npuls, nbins, nbits, nifs, nchans;
+  double az_start, za_start, src_raj, src_dej, tstart, tsamp, fch1, foff, refdm, period;
+  int32_t uses_frequency_table;
+  int32_t reversed; /* 1 when samples are delivered channel-reversed */
+  char rawdatafile[256];
+  char source_name[256];
+} gf_filterbank_header;
+
+/* The header part of read_filterbank (src/gaffa/io/filterbank.cpp:116-224,
+ * 335-348): fields, and the frequency of each delivered channel (up to
+ * capacity values; frequency_table may be NULL).  nbits 8, 16, 32 as the
+ * reference; packed 1-, 2- and 4-bit rows are accepted in addition. */
+int gf_filterbank_read_header(const char* path, int32_t channel_order,
+                              gf_filterbank_header* header, double* frequency_table,
+                              uint64_t capacity);
+/* Rows [row_begin, row_begin + nrows) into host memory, channel order as
+ * read_filterbank delivers it (src/gaffa/io/filterbank.cpp:243-333). */
+int gf_filterbank_read_host(const char* path, int32_t channel_order, uint64_t row_begin,
+                            uint64_t nrows, void* host_out);
+/* The same rows straight into device memory: the file is read into the two
+ * halves of a caller-owned pinned host buffer in turn, each half copied to the
+ * device while the other fills, and the channel reversal runs on the GPU.
+ * Returns once the last copy is issued; work is ordered on stream. */
+int gf_filterbank_load(const char* path, int32_t channel_order, uint64_t row_begin,
+                       uint64_t nrows, void* dev_out, void* host_bounce, uint64_t bounce_bytes,
+                       void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Preprocessing: running-median detrend + normalise                         */
 /* ------------------------------------------------------------------------ */

@@ -1350,3 +1350,38 @@ int gfo_remove_harmonics(const gfo_candidate* sorted, const gfo_harmonic_relatio
   *nout = k;
   return GFO_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* aligned spectrum: dedispersion.cpp:249-289                                */
+/* ------------------------------------------------------------------------ */
+
+int gfo_dedisperse_spectrum_u8(const uint8_t* in, uint64_t nsamples, uint64_t nchans,
+                               const double* freq, double dm, double ref, double tsamp,
+                               uint64_t cb, uint64_t ce, uint8_t* out, uint64_t* nout) {
+  if (nsamples == 0) return fail(GFO_EINVAL, "dedispersion requires at least one sample");
+  if (nchans == 0) return fail(GFO_EINVAL, "dedispersion requires at least one channel");
+  if (!(isfinite(ref) && ref > 0.0)) return fail(GFO_EINVAL, "reference frequency must be positive");
+  if (!(isfinite(tsamp) && tsamp > 0.0)) return fail(GFO_EINVAL, "tsamp must be positive");
+  if (cb >= ce) return fail(GFO_EINVAL, "channel range must be non-empty");
+  if (ce > nchans) return fail(GFO_EINVAL, "channel range exceeds sample channel count");
+  if (!isfinite(dm) || dm < 0.0) return fail(GFO_EINVAL, "dm must be finite and non-negative");
+  double fmin = freq[cb];
+  for (uint64_t c = cb; c < ce; ++c) {
+    if (!(isfinite(freq[c]) && freq[c] > 0.0))
+      return fail(GFO_EINVAL, "frequency values must be finite and positive");
+    if (freq[c] > ref)
+      return fail(GFO_EINVAL, "dedispersion requires selected frequencies <= reference frequency");
+    if (freq[c] < fmin) fmin = freq[c];
+  }
+  const int32_t maxd = gfo_delay_bins(dm, fmin, ref, tsamp);
+  if (maxd < 0) return fail(GFO_EINVAL, "dedispersion requires non-negative delays");
+  if ((uint64_t)maxd >= nsamples) return fail(GFO_EINVAL, "dedispersion valid output range is empty");
+  *nout = nsamples - (uint64_t)maxd;
+  if (!out) return GFO_OK;
+  const uint64_t nc = ce - cb;
+  for (uint64_t c = 0; c < nc; ++c) {
+    const int32_t d = gfo_delay_bins(dm, freq[cb + c], ref, tsamp);
+    for (uint64_t t = 0; t < *nout; ++t) out[t * nc + c] = in[(t + (uint64_t)d) * nchans + cb + c];
+  }
+  return GFO_OK;
+}

@@ -191,6 +191,27 @@ int gfo_select_candidates(const gfo_peak* peaks, uint64_t npeaks,
                           const gfo_candidate_options* options,
                           gfo_candidate** candidates, uint64_t* ncandidates);
 
+/* dedisperse_spectrum_cpu (dedispersion.cpp:249-289) for uint8 samples:
+ * out[t][c] = in[t + d(c)][chan_begin + c], t < nout (computed first with
+ * out == NULL). */
+int gfo_dedisperse_spectrum_u8(const uint8_t* in, uint64_t nsamples, uint64_t nchans,
+                               const double* freq, double dm, double ref_freq, double tsamp,
+                               uint64_t chan_begin, uint64_t chan_end, uint8_t* out,
+                               uint64_t* nout);
+
+/* ---- filterbank header (reference checker only: io/filterbank.cpp) ---- */
+typedef struct {
+  int64_t header_size;
+  int64_t nsamples;
+  int32_t telescope_id, machine_id, data_type, barycentric, pulsarcentric;
+  int32_t ibeam, nbeams, npuls, nbins, nbits, nifs, nchans;
+  double az_start, za_start, src_raj, src_dej, tstart, tsamp, fch1, foff, refdm, period;
+  int32_t uses_frequency_table;
+  int32_t reversed;
+  char rawdatafile[256];
+  char source_name[256];
+} gfo_filterbank_header; /* filterbank.h:33-65 FilterbankHeader */
+
 /* ---- harmonics (harmonic.cpp) ---- */
 typedef struct {
   double observation_seconds;

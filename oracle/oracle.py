@@ -279,6 +279,44 @@ class Oracle:
             C.c_double(observation_seconds), C.byref(o), C.byref(cp), C.byref(n)))
         return self._take(cp, n.value, CAND_DTYPE)
 
+    def dedisperse_spectrum(self, data, freq, dm, ref, tsamp, chan_begin=0, chan_end=None):
+        data = np.ascontiguousarray(data, np.uint8)
+        freq = np.ascontiguousarray(freq, np.float64)
+        ns, nc = data.shape
+        ce = nc if chan_end is None else chan_end
+        f = self._fn("dedisperse_spectrum_u8")
+        nout = C.c_uint64()
+        args = [data.ctypes.data_as(C.c_void_p), C.c_uint64(ns), C.c_uint64(nc),
+                freq.ctypes.data_as(C.c_void_p), C.c_double(dm), C.c_double(ref), C.c_double(tsamp),
+                C.c_uint64(chan_begin), C.c_uint64(ce)]
+        self._check(f(*args, None, C.byref(nout)))
+        out = np.zeros((nout.value, ce - chan_begin), np.uint8)
+        self._check(f(*args, out.ctypes.data_as(C.c_void_p), C.byref(nout)))
+        return out
+
+    def read_filterbank(self, path, preserve_file_order=False):
+        """read_filterbank (reference only): (header fields, frequencies, sample bytes)."""
+        class Hdr(C.Structure):
+            _fields_ = [("header_size", C.c_int64), ("nsamples", C.c_int64)] + \
+                [(n, C.c_int32) for n in ("telescope_id", "machine_id", "data_type", "barycentric",
+                                          "pulsarcentric", "ibeam", "nbeams", "npuls", "nbins", "nbits",
+                                          "nifs", "nchans")] + \
+                [(n, C.c_double) for n in ("az_start", "za_start", "src_raj", "src_dej", "tstart", "tsamp",
+                                           "fch1", "foff", "refdm", "period")] + \
+                [("uses_frequency_table", C.c_int32), ("reversed", C.c_int32),
+                 ("rawdatafile", C.c_char * 256), ("source_name", C.c_char * 256)]
+        h = Hdr()
+        freq = np.zeros(1 << 16, np.float64)
+        sp, n = C.c_void_p(), C.c_uint64()
+        self._check(self._fn("read_filterbank")(str(path).encode(), int(preserve_file_order), C.byref(h),
+                                                freq.ctypes.data_as(C.c_void_p), C.c_uint64(len(freq)),
+                                                C.byref(sp), C.byref(n)))
+        data = self._take(sp, n.value, np.dtype(np.uint8))
+        fields = {k: getattr(h, k) for k, _ in h._fields_ if k not in ("reversed",)}
+        fields["rawdatafile"] = h.rawdatafile.decode()
+        fields["source_name"] = h.source_name.decode()
+        return fields, freq[: h.nchans].copy(), data
+
     def flag_harmonics(self, candidates, observation_seconds, frequency_low_mhz, frequency_high_mhz,
                        max_harmonic=16, denominator_max=5, frequency_tolerance_bins=1.5,
                        phase_distance_max=1.0, dm_distance_max=3.0, use_snr_consistency=False,

@@ -12,6 +12,7 @@
 #include "gaffa/dedispersion.h"
 #include "gaffa/dm_search.h"
 #include "gaffa/ffa.h"
+#include "gaffa/filterbank.h"
 #include "gaffa/ffa_detection.h"
 #include "gaffa/ffa_plan.h"
 #include "gaffa/ffa_search.h"
@@ -26,6 +27,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <variant>
 #include <vector>
 
 namespace {
@@ -475,6 +477,52 @@ int gfr_remove_harmonics(const gfo_candidate* sorted, const gfo_harmonic_relatio
     const auto r = gaffa::remove_harmonics_cpu(in, max_candidates);
     for (size_t i = 0; i < r.size(); ++i) out[i] = sorted[static_cast<uint64_t>(r[i].frequency)];
     *nout = r.size();
+  });
+}
+
+int gfr_dedisperse_spectrum_u8(const uint8_t* in, uint64_t nsamples, uint64_t nchans, const double* freq,
+                               double dm, double ref, double tsamp, uint64_t cb, uint64_t ce, uint8_t* out,
+                               uint64_t* nout) {
+  return guarded([&] {
+    const auto r = gaffa::dedisperse_spectrum_cpu(
+        gaffa::HostSampleView<std::uint8_t>{std::span<const std::uint8_t>(in, nsamples * nchans),
+                                            gaffa::SampleShape{nsamples, 1, nchans}},
+        std::span<const double>(freq, nchans),
+        gaffa::SingleDmDedispersionPlan{.dm = dm, .ref_frequency_mhz = ref, .tsamp = tsamp,
+                                        .chan_begin = cb, .chan_end = ce});
+    *nout = r.shape.nsamples;
+    if (out) std::memcpy(out, r.data.data(), r.data.size());
+  });
+}
+
+// read_filterbank (io/filterbank.cpp:335-348): header, frequencies and the
+// samples' bytes (malloc'd, released with gfr_free).
+int gfr_read_filterbank(const char* path, int preserve, gfo_filterbank_header* h, double* freq,
+                        uint64_t capacity, void** samples, uint64_t* nbytes) {
+  return guarded([&] {
+    gaffa::FilterbankReadOptions o;
+    if (preserve) o.channel_order = gaffa::ChannelOrderPolicy::PreserveFileOrder;
+    const auto d = gaffa::read_filterbank(path, o);
+    const auto& x = d.header;
+    std::memset(h, 0, sizeof *h);
+    h->header_size = x.header_size;
+    h->nsamples = x.nsamples;
+    h->telescope_id = x.telescope_id; h->machine_id = x.machine_id; h->data_type = x.data_type;
+    h->barycentric = x.barycentric; h->pulsarcentric = x.pulsarcentric; h->ibeam = x.ibeam;
+    h->nbeams = x.nbeams; h->npuls = x.npuls; h->nbins = x.nbins; h->nbits = x.nbits; h->nifs = x.nifs;
+    h->nchans = x.nchans;
+    h->az_start = x.az_start; h->za_start = x.za_start; h->src_raj = x.src_raj; h->src_dej = x.src_dej;
+    h->tstart = x.tstart; h->tsamp = x.tsamp; h->fch1 = x.fch1; h->foff = x.foff; h->refdm = x.refdm;
+    h->period = x.period;
+    h->uses_frequency_table = x.uses_frequency_table ? 1 : 0;
+    std::strncpy(h->rawdatafile, x.rawdatafile.c_str(), sizeof h->rawdatafile - 1);
+    std::strncpy(h->source_name, x.source_name.c_str(), sizeof h->source_name - 1);
+    for (uint64_t i = 0; i < capacity && i < x.frequency_table.size(); ++i) freq[i] = x.frequency_table[i];
+    std::visit([&](const auto& v) {
+      *nbytes = v.size() * sizeof(v[0]);
+      *samples = std::malloc(*nbytes ? *nbytes : 1);
+      if (*nbytes) std::memcpy(*samples, v.data(), *nbytes);
+    }, d.samples);
   });
 }
 

@@ -10,6 +10,9 @@ from the reference's own functions through ``oracle/ref_shim.cpp``:
 Writes
   ref_small.npz            small seeded cases for every hot-path function
   ref_harmonic.npz         seeded candidate lists through flag_harmonics_cpu
+  ref_spectrum.npz         aligned single-DM spectra (dedisperse_spectrum_cpu)
+  ref_filterbank.npz       read_filterbank of the reference's tests/data/basetest.fil:
+                           header fields, frequencies, sample digest, first rows
   ref_plain_end_to_end.npz the full plain end-to-end workload (256 ch, 2^18
                            samples, 512 DMs): digests of the dedispersed block
                            and of all raw peaks, the candidate list and the
@@ -234,6 +237,37 @@ def harmonic_cases(ref: Oracle) -> dict:
     return out
 
 
+def spectrum_cases(ref: Oracle) -> dict:
+    obs = synth.Observation(nchans=48, nsamples=3000, tsamp=1e-3, f_low=1200.0, f_high=1500.0, seed=5,
+                            pulsars=[synth.Pulsar(0.2, 60.0, 0.05, 40.0)])
+    data = synth.generate(obs)
+    f = obs.frequencies
+    out = {"sp_data": data, "sp_freq": f}
+    out["sp_full"] = ref.dedisperse_spectrum(data, f, 60.0, f.max(), obs.tsamp)
+    out["sp_sub"] = ref.dedisperse_spectrum(data, f, 37.5, f.max(), obs.tsamp, 5, 41)
+    out["sp_zero"] = ref.dedisperse_spectrum(data, f, 0.0, f.max(), obs.tsamp)
+    return out
+
+
+def filterbank_cases(ref: Oracle) -> dict:
+    path = Path(ref_dir()) / "tests" / "data" / "basetest.fil"
+    out = {}
+    for tag, preserve in (("asc", False), ("file", True)):
+        h, f, data = ref.read_filterbank(path, preserve)
+        for k, v in h.items():
+            out[f"{tag}_h_{k}"] = np.array(v)
+        out[f"{tag}_freq"] = f
+        out[f"{tag}_digest"] = np.array(digest(data))
+        out[f"{tag}_head"] = data[: 64 * 1024]
+    return out
+
+
+def ref_dir() -> str:
+    import re
+    make = (ROOT / "oracle" / "Makefile").read_text()
+    return re.search(r"^REF_DIR \?= (.+)$", make, re.M).group(1).strip()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-plain", action="store_true")
@@ -241,6 +275,8 @@ def main() -> None:
     args = ap.parse_args()
     ref = Oracle("reference")
     np.savez_compressed(OUT / "ref_harmonic.npz", **harmonic_cases(ref))
+    np.savez_compressed(OUT / "ref_spectrum.npz", **spectrum_cases(ref))
+    np.savez_compressed(OUT / "ref_filterbank.npz", **filterbank_cases(ref))
     if not args.skip_small:
         np.savez_compressed(OUT / "ref_small.npz", **small_cases(ref))
     if not args.skip_plain:
