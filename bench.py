@@ -37,6 +37,9 @@ METRIC = "DM-trial·samples/s searched"
 UNIT = "DM-trial·samples/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) one FFA search moves per DM-trial series, from the
+# ncu capture summarised in this file (survey-size workload only)
+FFA_TRAFFIC_FILE = ROOT / "profiles" / "ffa_search_kernel_survey_size.md"
 
 
 def parse_args():
@@ -121,6 +124,19 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def ffa_traffic_per_series(workload: str):
+    """traffic_bytes_per_series recorded in the FFA profile summary."""
+    if workload != "survey_size":
+        return None
+    try:
+        for line in FFA_TRAFFIC_FILE.read_text().splitlines():
+            if line.strip().startswith("traffic_bytes_per_series:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
 
 
 def measured_hbm_gbs():
@@ -304,10 +320,21 @@ def main():
     units_per_launch = units / launches_per_step
     alg = algorithmic_bytes(dominant, cfg, ds, units_per_launch)
     achieved = alg / (per_launch_ms / 1e3) / 1e9
+    traffic = None
+    series_per_launch = units_per_launch / ds.nout
+    if dominant == "ffa" and ffa_traffic_per_series(cfg.name) is not None:
+        traffic = ffa_traffic_per_series(cfg.name) * series_per_launch
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": dominant, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": traffic, "kernel": dominant, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_ms,
                 "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in totals.items()}}
+    # the compute roofs that actually bind these kernels
+    if "ffa" in totals:
+        per_series = float(sum(int(t["rows"]) * int(t["bins"]) * max(1, int(t["rows"]) - 1).bit_length()
+                               for t in ds.plan.tasks))
+        roofline["ffa_element_levels_per_s"] = per_series * cfg.ndm / (totals["ffa"] / args.steps / 1e3)
+    if "dedisperse" in totals:
+        roofline["dedisperse_adds_per_s"] = float(cfg.ndm) * obs.nchans * ds.nout / (totals["dedisperse"] / args.steps / 1e3)
 
     e2e = None
     host = None
@@ -316,7 +343,8 @@ def main():
         host.copy_(raw)
         step(host)
         ms_e2e, _ = timed(host, args.steps)
-        d2h = int(res.gpu_launches * 0) + len(res.peaks) * 24 + 16 + ds.fold_nbin * 12
+        # peak records + counters + the folded profile (float) and exposure (double)
+        d2h = len(res.peaks) * 24 + 16 + ds.fold_nbin * 12
         e2e = {"value": units * world / (ms_e2e / 1e3), "unit": UNIT, "ms_per_step": ms_e2e,
                "h2d_bytes_per_step": int(raw.numel()), "d2h_bytes_per_step": d2h}
 
@@ -338,7 +366,7 @@ def main():
                        "ndm": cfg.ndm, "nout": ds.nout, "dedispersion": cfg.dedispersion,
                        "ffa_tasks": ds.plan.task_count, "width_trials": list(ds.plan.width_trials),
                        "dm_batch": ds.dm_batch, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (34 GB filterbank)", "peaks": len(res.peaks),
+                       "l2": f"inputs larger than L2 ({raw.numel() / 1e9:.1f} GB filterbank)", "peaks": len(res.peaks),
                        "candidates": len(res.candidates)},
             "e2e": e2e,
             "gpu_launches": res.gpu_launches * args.steps,
