@@ -177,6 +177,15 @@ _SIGNATURES = [
     ("gf_filterbank_read_header", C.c_int, [C.c_char_p, i32, C.POINTER(FilterbankHeader), vp, u64]),
     ("gf_filterbank_read_host", C.c_int, [C.c_char_p, i32, u64, u64, vp]),
     ("gf_filterbank_load", C.c_int, [C.c_char_p, i32, u64, u64, vp, vp, u64, vp]),
+    ("gf_fold_spectrum", C.c_int, [vp, i32, u64, u64, dbl, dbl, u64, u64, u64, u64, vp, vp, vp, vp]),
+    ("gf_project_folded_cube", C.c_int, [vp, vp, u64, u64, u64, vp, vp, vp, vp]),
+    ("gf_prop_conv_forward", C.c_int, [vp, vp, vp, vp, i32, i32, i32, i32, i32, i32, vp]),
+    ("gf_prop_conv_backward", C.c_int, [vp, vp, vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, vp]),
+    ("gf_prop_head", C.c_int, [vp, vp, vp, i32, i32, i32, i32, vp, C.c_float, vp, vp, vp, vp, vp, vp]),
+    ("gf_prop_adam", C.c_int, [vp, vp, vp, vp, vp, u64, C.c_float, C.c_float, C.c_float, C.c_float, i32,
+                               C.c_float, vp]),
+    ("gf_prop_features", C.c_int, [vp, u64, u64, dbl, vp, i32, vp, vp]),
+    ("gf_prop_downsample", C.c_int, [vp, u64, u64, i32, u64, vp, u64, vp]),
     ("gf_flag_harmonics", C.c_int, [vp, u64, C.POINTER(HarmonicContext), C.POINTER(HarmonicOptions), vp, vp]),
     ("gf_remove_harmonics", C.c_int, [vp, vp, u64, u64, vp, C.POINTER(u64)]),
 ]

@@ -16,7 +16,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libgaffa_b200.so"
-SOURCES = ["host.cpp", "dedisperse.cu", "preprocess.cu", "ffa.cu", "fold.cu", "synth.cu", "filterbank.cu"]
+SOURCES = ["host.cpp", "dedisperse.cu", "preprocess.cu", "ffa.cu", "fold.cu", "synth.cu", "filterbank.cu", "proposal.cu"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

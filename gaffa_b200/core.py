@@ -462,6 +462,52 @@ def load_filterbank(path, preserve_file_order: bool = False, row_begin: int = 0,
     return h, freq, out
 
 
+def fold_spectrum(spectrum: torch.Tensor, period: float, tsamp: float, nbin: int, subint_samples: int,
+                  start_sample: int = 0, output_channels: int = 0, stream=None):
+    """fold_spectrum_cpu (src/gaffa/folding.cpp:300-420) on a device spectrum
+    [nsamples][nchans]: (cube [nsubint][nout][nbin] float, exposure
+    [nsubint][nbin] double), both on the device."""
+    if spectrum.dim() != 2 or not spectrum.is_cuda:
+        raise ValueError("spectrum must be a 2-D CUDA tensor [nsamples][nchans]")
+    elem = {torch.uint8: 1, torch.int16: 2, torch.uint16: 2, torch.float32: 4}.get(spectrum.dtype)
+    if elem is None:
+        raise TypeError("spectrum dtype must be uint8, uint16 or float32")
+    sp = spectrum.contiguous()
+    ns, nc = sp.shape
+    nout = output_channels or nc
+    nsub = -(-ns // subint_samples) if subint_samples > 0 else 0
+    cube = torch.empty((max(nsub, 1), nout, nbin), dtype=torch.float32, device=sp.device)
+    expo = torch.empty((max(nsub, 1), nbin), dtype=torch.float64, device=sp.device)
+    status = torch.empty(1, dtype=torch.int32, device=sp.device)
+    s = stream if stream is not None else torch.cuda.current_stream(sp.device)
+    check(_lib.lib().gf_fold_spectrum(ptr(sp), elem, ns, nc, period, tsamp, nbin, subint_samples, start_sample,
+                                      output_channels, ptr(cube), ptr(expo), ptr(status), C.c_void_p(s.cuda_stream)))
+    if int(status.item()) & _lib.STATUS_NONFINITE:
+        raise ValueError("fold spectrum must contain only finite samples")
+    return cube, expo
+
+
+def fold_dedispersed_spectrum(filterbank: torch.Tensor, frequency_mhz, dm: float, period: float, tsamp: float,
+                              nbin: int, tsubint: float = 10.0, output_channels: int = 0):
+    """fold_dedispersed_spectrum (src/gaffa/folding.cpp:408-438): aligned
+    spectrum at dm, folded into subints of round(tsubint / tsamp) samples, and
+    the projections.  Returns a dict of device tensors."""
+    if not (math.isfinite(tsubint) and tsubint > 0.0):
+        raise ValueError("fold tsubint must be finite and positive")
+    sub = max(1, int(round(tsubint / tsamp)))
+    spec = dedisperse_spectrum(filterbank, frequency_mhz, dm, tsamp)
+    cube, expo = fold_spectrum(spec, period, tsamp, nbin, sub, 0, output_channels)
+    nsub, nch, _ = cube.shape
+    prof = torch.empty(nbin, dtype=torch.float32, device=cube.device)
+    fp = torch.empty((nch, nbin), dtype=torch.float32, device=cube.device)
+    tp = torch.empty((nsub, nbin), dtype=torch.float32, device=cube.device)
+    s = torch.cuda.current_stream(cube.device)
+    check(_lib.lib().gf_project_folded_cube(ptr(cube), ptr(expo), nsub, nch, nbin, ptr(prof), ptr(fp), ptr(tp),
+                                            C.c_void_p(s.cuda_stream)))
+    return {"cube": cube, "exposure": expo, "profile": prof, "freq_phase": fp, "time_phase": tp,
+            "tsubint": sub * tsamp}
+
+
 def harmonic_options(max_harmonic: int = 16, denominator_max: int = 5, frequency_tolerance_bins: float = 1.5,
                      phase_distance_max: float = 1.0, dm_distance_max: float = 3.0,
                      use_snr_consistency: bool = False, snr_distance_max: float = 3.0):

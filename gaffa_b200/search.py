@@ -119,8 +119,21 @@ class DmSearch:
     def stage(self, filterbank) -> torch.Tensor:
         return self.dedisp.stage(filterbank)
 
-    def search_staged(self, staged: torch.Tensor, timers: dict | None = None) -> tuple:
-        """Runs every DM batch; returns (raw peaks, kernel launches).
+    def batches(self, dm_ranges=None):
+        """(first DM, count) of every batch; dm_ranges (optional) restricts the
+        search to [begin, end) ranges of DM indices, begin a multiple of the
+        dedispersion granularity."""
+        ranges = [(0, self.ndm)] if dm_ranges is None else dm_ranges
+        g = self.dedisp.batch_granularity
+        for begin, end in ranges:
+            if begin % g or not 0 <= begin < end <= self.ndm:
+                raise ValueError(f"DM range ({begin}, {end}) must start at a multiple of {g} within [0, ndm]")
+            for b0 in range(begin, end, self.dm_batch):
+                yield b0, min(self.dm_batch, end - b0)
+
+    def search_staged(self, staged: torch.Tensor, timers: dict | None = None, dm_ranges=None) -> tuple:
+        """Runs every DM batch (or the batches of dm_ranges); returns (raw
+        peaks, kernel launches).
 
         timers (optional) collects CUDA events around each stage's launches:
         dedisperse, preprocess, prepare, ffa."""
@@ -128,8 +141,7 @@ class DmSearch:
         launches = 0
         dd_kernels = 1 if self.dedisp.algorithm == "brute" else 2
         ffa_kernels = self.ffa.kernel_launches
-        for b0 in range(0, self.ndm, self.dm_batch):
-            cnt = min(self.dm_batch, self.ndm - b0)
+        for b0, cnt in self.batches(dm_ranges):
             with _StageTimer(timers, "dedisperse"):
                 dd = self.dedisp.run(staged, b0, cnt, out=self._series, out_stride=self.out_stride,
                                      workspace=self._workspace)
@@ -158,14 +170,15 @@ class DmSearch:
         row = dd[dm_index - b0, : self.nout]
         return core.fold_time_series(row, period, self.tsamp, self.fold_nbin)
 
-    def run(self, filterbank, observation_seconds: float | None = None, timers: dict | None = None) -> SearchResult:
+    def run(self, filterbank, observation_seconds: float | None = None, timers: dict | None = None,
+            dm_ranges=None) -> SearchResult:
         t = {}
         t0 = time.perf_counter()
         with _StageTimer(timers, "stage"):
             staged = self.stage(filterbank)
         torch.cuda.synchronize(self.device)
         t1 = time.perf_counter()
-        peaks, launches = self.search_staged(staged, timers)
+        peaks, launches = self.search_staged(staged, timers, dm_ranges)
         t2 = time.perf_counter()
         peaks = core.sort_peaks(peaks)
         tobs = self.nsamples * self.tsamp if observation_seconds is None else observation_seconds

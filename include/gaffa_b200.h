@@ -451,6 +451,66 @@ int gf_remove_harmonics(const gf_candidate* sorted, const gf_harmonic_relation* 
                         uint64_t n, uint64_t max_candidates, gf_candidate* out,
                         uint64_t* nout);
 
+/* Spectrum folding.  Replaces fold_spectrum_cpu (src/gaffa/folding.cpp:
+ * 300-420): a device time-major spectrum [nsamples][nchans] (elem_bytes 1, 2
+ * or 4: uint8, uint16, float) folded at `period` into
+ * cube[nsubint][nout][nbin] (float, sums / exposure) and
+ * exposure[nsubint][nbin] (double), nsubint = ceil(nsamples / subint_samples),
+ * nout = output_channels (0: nchans; adjacent input channels are averaged).
+ * nbin <= 256.  dev_status receives GF_STATUS_NONFINITE for non-finite float
+ * input.  FP64 sums in a different order from the reference: the cube agrees
+ * to FP64 rounding. */
+int gf_fold_spectrum(const void* dev_in, int32_t elem_bytes, uint64_t nsamples, uint64_t nchans,
+                     double period, double tsamp, uint64_t nbin, uint64_t subint_samples,
+                     uint64_t start_sample, uint64_t output_channels, float* dev_cube,
+                     double* dev_exposure, uint32_t* dev_status, void* stream);
+/* Replaces project_folded_cube (src/gaffa/folding.cpp:237-296): profile
+ * [nbin], freq_phase [nchans][nbin] and time_phase [nsubint][nbin] of a
+ * folded cube, in the reference's summation order. */
+int gf_project_folded_cube(const float* dev_cube, const double* dev_exposure, uint64_t nsubint,
+                           uint64_t nchans, uint64_t nbin, float* dev_profile, float* dev_freq_phase,
+                           float* dev_time_phase, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Learned DM/period proposal (no counterpart in the reference)              */
+/* ------------------------------------------------------------------------ */
+/* A small 1-D convolutional network that scores coarse DM trials per period
+ * octave, so full-resolution search can run on the best-scoring DM windows
+ * only; the exhaustive search stays the fallback.  Tensors are [batch]
+ * [channels][length], activations and weights bf16 (uint16 storage),
+ * accumulation and gradients fp32. */
+
+/* y = act(bias + conv(x, w)), w [cout][cin][ksize], zero padding ksize/2,
+ * relu 0/1.  cin <= 64, ksize odd <= 9. */
+int gf_prop_conv_forward(const void* x, const void* w, const float* bias, void* y, int32_t batch,
+                         int32_t cin, int32_t cout, int32_t length, int32_t ksize, int32_t relu,
+                         void* stream);
+/* Backward of a ReLU conv layer: dy (fp32, overwritten by dy * (y_act > 0)
+ * when y_act != NULL) -> dw, db accumulated (+=), dx written when non-NULL. */
+int gf_prop_conv_backward(const float* dy, const void* y_act, const void* x, const void* w, float* dx,
+                          float* dw, float* db, int32_t batch, int32_t cin, int32_t cout, int32_t length,
+                          int32_t ksize, void* stream);
+/* Head (1x1 conv channels -> 1), per-octave log-mean-exp pooling over
+ * length/octaves bins (<= 64), and with labels the positive-weighted binary
+ * cross-entropy (added to *loss) and its gradients (dy written, dwh, dbh
+ * accumulated). */
+int gf_prop_head(const void* y, const float* wh, const float* bh, int32_t batch, int32_t channels,
+                 int32_t length, int32_t octaves, const float* labels, float pos_weight,
+                 float* logits, float* loss, float* dy, float* dwh, float* dbh, void* stream);
+/* One Adam step on fp32 master weights (grad scaled by grad_scale); refreshes
+ * the bf16 copy when param_bf16 != NULL. */
+int gf_prop_adam(float* param, const float* grad, float* m, float* v, void* param_bf16, uint64_t n,
+                 float lr, float beta1, float beta2, float eps, int32_t step, float grad_scale,
+                 void* stream);
+/* Harmonic-summed spectral features: power [nseries][nfreq] (white noise
+ * mean 1 per bin, bin k at k*df Hz) -> feat bf16 [nseries][nbins] over the
+ * log frequency bin edges[0..nbins]. */
+int gf_prop_features(const float* power, uint64_t nseries, uint64_t nfreq, double df,
+                     const float* edges, int32_t nbins, void* feat, void* stream);
+/* out[r][t] = sum of `factor` consecutive uint32 samples of in[r] (float). */
+int gf_prop_downsample(const uint32_t* in, uint64_t in_stride, uint64_t nrows, int32_t factor,
+                       uint64_t nout, float* out, uint64_t out_stride, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Folding                                                                   */
 /* ------------------------------------------------------------------------ */

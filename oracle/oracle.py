@@ -317,6 +317,24 @@ class Oracle:
         fields["source_name"] = h.source_name.decode()
         return fields, freq[: h.nchans].copy(), data
 
+    def fold_dedispersed_spectrum(self, spectrum, period, tsamp, nbin, tsubint=10.0, output_channels=0):
+        """fold_dedispersed_spectrum_view_cpu of a uint8 [ns][nc] spectrum (reference only)."""
+        x = np.ascontiguousarray(spectrum, np.uint8)
+        ns, nc = x.shape
+        f = self._fn("fold_dedispersed_spectrum_u8")
+        nsub = C.c_uint64()
+        args = [x.ctypes.data_as(C.c_void_p), C.c_uint64(ns), C.c_uint64(nc), C.c_double(period),
+                C.c_double(tsamp), C.c_uint64(nbin), C.c_double(tsubint), C.c_uint64(output_channels),
+                C.byref(nsub)]
+        self._check(f(*args, None, None, None, None, None))
+        nout = output_channels or nc
+        out = dict(cube=np.zeros((nsub.value, nout, nbin), np.float32),
+                   exposure=np.zeros((nsub.value, nbin), np.float64), profile=np.zeros(nbin, np.float32),
+                   freq_phase=np.zeros((nout, nbin), np.float32), time_phase=np.zeros((nsub.value, nbin), np.float32))
+        self._check(f(*args, *[out[k].ctypes.data_as(C.c_void_p) for k in
+                               ("cube", "exposure", "profile", "freq_phase", "time_phase")]))
+        return out
+
     def flag_harmonics(self, candidates, observation_seconds, frequency_low_mhz, frequency_high_mhz,
                        max_harmonic=16, denominator_max=5, frequency_tolerance_bins=1.5,
                        phase_distance_max=1.0, dm_distance_max=3.0, use_snr_consistency=False,

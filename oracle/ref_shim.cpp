@@ -526,4 +526,28 @@ int gfr_read_filterbank(const char* path, int preserve, gfo_filterbank_header* h
   });
 }
 
+// fold_dedispersed_spectrum_view_cpu (folding.cpp:408-438) of a uint8
+// [ns][nc] spectrum; outputs sized by the caller from nsubint (first call with
+// cube == NULL returns it).
+int gfr_fold_dedispersed_spectrum_u8(const uint8_t* in, uint64_t ns, uint64_t nc, double period, double tsamp,
+                                     uint64_t nbin, double tsubint, uint64_t out_ch, uint64_t* nsubint,
+                                     float* cube, double* exposure, float* profile, float* freq_phase,
+                                     float* time_phase) {
+  return guarded([&] {
+    const auto r = gaffa::fold_dedispersed_spectrum_view_cpu(
+        gaffa::HostSampleView<std::uint8_t>{std::span<const std::uint8_t>(in, ns * nc),
+                                            gaffa::SampleShape{ns, 1, nc}},
+        tsamp,
+        gaffa::FoldDedispersedSpectrumOptions{.period = period, .nbin = nbin, .tsubint = tsubint,
+                                              .output_channels = out_ch});
+    *nsubint = r.nsubint;
+    if (!cube) return;
+    std::memcpy(cube, r.cube.data.data(), r.cube.data.size() * sizeof(float));
+    std::memcpy(exposure, r.cube.exposure.data(), r.cube.exposure.size() * sizeof(double));
+    std::memcpy(profile, r.profile.data(), r.profile.size() * sizeof(float));
+    std::memcpy(freq_phase, r.freq_phase.data(), r.freq_phase.size() * sizeof(float));
+    std::memcpy(time_phase, r.time_phase.data(), r.time_phase.size() * sizeof(float));
+  });
+}
+
 }  // extern "C"

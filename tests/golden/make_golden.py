@@ -246,6 +246,11 @@ def spectrum_cases(ref: Oracle) -> dict:
     out["sp_full"] = ref.dedisperse_spectrum(data, f, 60.0, f.max(), obs.tsamp)
     out["sp_sub"] = ref.dedisperse_spectrum(data, f, 37.5, f.max(), obs.tsamp, 5, 41)
     out["sp_zero"] = ref.dedisperse_spectrum(data, f, 0.0, f.max(), obs.tsamp)
+    # fold of the aligned spectrum at the pulsar's period
+    for tag, kw in (("fold", dict(nbin=32, tsubint=0.5)), ("fold_ch", dict(nbin=24, tsubint=0.7, output_channels=12))):
+        r = ref.fold_dedispersed_spectrum(out["sp_full"], 0.2, obs.tsamp, **kw)
+        for k, v in r.items():
+            out[f"{tag}_{k}"] = v
     return out
 
 

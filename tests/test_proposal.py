@@ -1,0 +1,108 @@
+"""Learned DM/period proposal: the network's CUDA forward/backward against the
+float64 CPU oracle (oracle/proposal_oracle.py), the oracle against finite
+differences, the label/selection helpers, and (GPU) a small training run that
+must beat the untrained network."""
+import numpy as np
+import pytest
+
+from oracle import proposal_oracle as po
+
+LAYERS = ((32, 64, 9), (64, 64, 9), (64, 32, 9))
+OCT = 7
+
+
+def small_net(rng, layers=((4, 6, 5), (6, 3, 3)), octaves=2, L=16):
+    ws = [rng.normal(0, 0.5, (co, ci, k)) for ci, co, k in layers]
+    bs = [rng.normal(0, 0.1, co) for _, co, _ in layers]
+    wh = rng.normal(0, 0.5, layers[-1][1])
+    bh = np.array([0.1])
+    feat = rng.normal(0, 1, (3, layers[0][0], L))
+    labels = (rng.random((3, octaves)) < 0.4).astype(np.float64)
+    return feat, ws, bs, wh, bh, labels
+
+
+def test_oracle_gradients_match_finite_differences():
+    rng = np.random.default_rng(0)
+    feat, ws, bs, wh, bh, labels = small_net(rng)
+    loss, dws, dbs, dwh, dbh, _ = po.loss_and_grads(feat, ws, bs, wh, bh, labels, 3.0, 2, rounding=False)
+    eps = 1e-6
+
+    def f():
+        return po.loss_and_grads(feat, ws, bs, wh, bh, labels, 3.0, 2, rounding=False)[0]
+
+    for arr, grad in [(ws[0], dws[0]), (ws[1], dws[1]), (bs[0], dbs[0]), (wh, dwh), (bh, dbh)]:
+        flat, gflat = arr.reshape(-1), grad.reshape(-1)
+        for i in rng.choice(len(flat), size=min(6, len(flat)), replace=False):
+            old = flat[i]
+            flat[i] = old + eps
+            up = f()
+            flat[i] = old - eps
+            dn = f()
+            flat[i] = old
+            assert abs((up - dn) / (2 * eps) - gflat[i]) < 1e-6 * max(1.0, abs(gflat[i]))
+
+
+def test_bf16_rounding_matches_torch():
+    torch = pytest.importorskip("torch")
+    x = np.random.default_rng(1).normal(0, 3, 1000).astype(np.float32)
+    ref = torch.from_numpy(x).to(torch.bfloat16).to(torch.float64).numpy()
+    assert np.array_equal(po.bf16_round(x), ref)
+
+
+def test_labels_windows_and_octaves():
+    from gaffa_b200 import _lib, proposal
+    c = np.zeros(3, _lib.CAND_DTYPE)
+    c["dm"] = [0.0, 500.0, 1000.0]
+    c["period"] = [0.15, 1.0, 12.0]
+    c["snr"] = [9.0, 7.0, 30.0]
+    y = proposal.labels_from_candidates(c, 1000.0, 8.0)
+    assert y.sum() == 2 and y[0, 6] == 1 and y[63, 0] == 1
+    assert list(proposal.octave_of_period([0.1, 0.25, 0.5, 12.7])) == [6, 5, 4, 0]
+    w = proposal.window_dm_indices([0, 63], 2048, 1000.0 / 2047, 1000.0)
+    assert w[0] == 0 and w[-1] == 2047 and len(w) < 2048 // 16
+    assert proposal.recall(c, [0], 1000.0, 8.0) == (1, 2)
+
+
+@pytest.mark.gpu
+def test_cuda_forward_and_gradients_match_oracle():
+    import torch
+    from gaffa_b200 import proposal
+    rng = np.random.default_rng(2)
+    net = proposal.ProposalNet(seed=3)
+    B, L = 3, proposal.NBINS
+    feat = torch.from_numpy(rng.normal(0, 1, (B, 32, L)).astype(np.float32)).cuda().to(torch.bfloat16)
+    labels = torch.from_numpy((rng.random((B, OCT)) < 0.3).astype(np.float32)).cuda()
+    loss, grads, logits = net.loss_and_grads(feat, labels, 7.0)
+    ws = [w.cpu().double().numpy() for w in net.w]
+    bs = [b.cpu().double().numpy() for b in net.b]
+    ref = po.loss_and_grads(feat.float().cpu().numpy(), ws, bs, net.wh.cpu().double().numpy(),
+                            net.bh.cpu().double().numpy(), labels.cpu().double().numpy(), 7.0, OCT)
+    np.testing.assert_allclose(logits.cpu().numpy(), ref[5], rtol=2e-2, atol=2e-2)
+    assert abs(loss - ref[0]) < 1e-2 * abs(ref[0])
+    nl = len(proposal.LAYERS)
+    pairs = list(zip(grads[:nl], ref[1])) + list(zip(grads[nl:2 * nl], ref[2])) + [(grads[2 * nl], ref[3]),
+                                                                                     (grads[2 * nl + 1], ref[4])]
+    for g, r in pairs:
+        g = g.cpu().double().numpy()
+        assert np.linalg.norm(g - r) <= 3e-2 * np.linalg.norm(r) + 1e-9
+
+
+@pytest.mark.gpu
+def test_training_reduces_loss_on_fixed_batch():
+    import torch
+    from gaffa_b200 import proposal
+    rng = np.random.default_rng(4)
+    net = proposal.ProposalNet(seed=5)
+    B = 32
+    feat = torch.from_numpy(rng.normal(0, 1, (B, 32, proposal.NBINS)).astype(np.float32))
+    labels = np.zeros((B, OCT), np.float32)
+    labels[: B // 2, 3] = 1.0
+    feat[: B // 2, :, 3 * 64 + 20] += 4.0      # a feature the positives carry
+    feat = feat.cuda().to(torch.bfloat16)
+    y = torch.from_numpy(labels).cuda()
+    first = net.train_step(feat, y, 5.0, 3e-3)
+    for _ in range(60):
+        last = net.train_step(feat, y, 5.0, 3e-3)
+    assert last < 0.5 * first
+    logits = net.forward(feat)
+    assert (logits[: B // 2, 3].min() > logits[B // 2:, 3].max()).item()

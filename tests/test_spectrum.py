@@ -56,3 +56,38 @@ def test_cuda_spectrum_float_and_errors(golden):
         core.dedisperse_spectrum(x, f, -1.0, 1e-3)                 # negative DM
     with pytest.raises(ValueError):
         core.dedisperse_spectrum(x, f, 60.0, 1e-3, ref_frequency_mhz=1300.0)
+
+
+FOLD_RTOL = 1e-6  # FP64 sums in a different order from the reference
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag,kw", [("fold", dict(nbin=32, tsubint=0.5)),
+                                    ("fold_ch", dict(nbin=24, tsubint=0.7, output_channels=12))])
+def test_cuda_fold_dedispersed_spectrum_matches_reference(golden, tag, kw):
+    """fold_dedispersed_spectrum_view_cpu of the aligned spectrum (folding.cpp:408-438):
+    cube and exposure, then the profile / frequency-phase / time-phase projections."""
+    import torch
+    from gaffa_b200 import core
+    x = torch.from_numpy(golden["sp_data"]).cuda()
+    r = core.fold_dedispersed_spectrum(x, golden["sp_freq"], 60.0, 0.2, 1e-3, **kw)
+    np.testing.assert_allclose(r["exposure"].cpu().numpy(), golden[f"{tag}_exposure"], rtol=1e-12)
+    for k in ("cube", "profile", "freq_phase", "time_phase"):
+        np.testing.assert_allclose(r[k].cpu().numpy(), golden[f"{tag}_{k}"], rtol=FOLD_RTOL, atol=1e-5)
+
+
+@pytest.mark.gpu
+def test_cuda_fold_spectrum_rejects_bad_arguments(golden):
+    import torch
+    from gaffa_b200 import core
+    x = torch.from_numpy(golden["sp_full"]).cuda()
+    with pytest.raises(ValueError):
+        core.fold_spectrum(x, 0.2, 1e-3, 32, 0)                          # subint_samples == 0
+    with pytest.raises(ValueError):
+        core.fold_spectrum(x, 0.2, 1e-3, 32, 100, output_channels=7)     # 48 % 7 != 0
+    with pytest.raises(ValueError):
+        core.fold_spectrum(x, -0.2, 1e-3, 32, 100)
+    bad = x.float()
+    bad[3, 5] = float("nan")
+    with pytest.raises(ValueError, match="finite"):
+        core.fold_spectrum(bad, 0.2, 1e-3, 32, 100)
