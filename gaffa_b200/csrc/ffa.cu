@@ -677,6 +677,13 @@ SearchKernel search_kernel_for(uint32_t nb) {
 
 using namespace gf;
 
+// Shared-memory geometry of the launches of one NB = ceil(bins/32): row pitch,
+// rows per buffer, column-block sizes and the dynamic shared memory.
+struct FfaGeometry {
+  uint32_t pitch = 0, max_rows = 0, block_rows = 0, final_rows = 0, levels = 0, front = 0;
+  size_t smem_bytes = 0;
+};
+
 struct FfaClass {
   int cluster = 1;             // CTAs cooperating on one (series, task)
   uint32_t nb = 1;             // ceil(bins / 32) of every task of the class
@@ -703,11 +710,10 @@ struct gf_ffa_program {
   uint64_t nsamples = 0;
   uint64_t prep_stride = 0;
   uint32_t max_bins = 0, max_width = 0;
-  uint32_t pitch = 0, max_rows = 0, block_rows = 0, final_rows = 0, levels = 0, front = 0;
+  FfaGeometry geo[17];         // by NB (1..16)
   uint64_t halo = 0;
   uint64_t max_series = 0;
   uint64_t scratch_floats = 0;
-  size_t smem_bytes = 0;
   DeviceBlob tasks_d, trials_d, octaves_d, sub_meta_d, sub_offset_d, col_meta_d, blocks_d, passes_d;
 };
 
@@ -879,15 +885,15 @@ void build_column_block(uint32_t bins, uint32_t xa, uint32_t xn, uint32_t s0, ui
 }
 
 // All column passes of a task split at depth dS (> 0).
-void build_task_passes(gf_ffa_program& P, TaskDev& d) {
-  const uint32_t dS = d.split_depth, K = P.levels;
+void build_task_passes(gf_ffa_program& P, const FfaGeometry& g, TaskDev& d) {
+  const uint32_t dS = d.split_depth, K = g.levels;
   d.pass_begin = static_cast<uint32_t>(P.passes.size());
   uint32_t depth = dS;
   while (true) {
     const uint32_t dn = cut_after(depth, dS, K);
     const uint32_t levels = depth - dn;
     const bool final_pass = dn == 0;
-    const uint32_t R = final_pass ? P.final_rows : P.block_rows;
+    const uint32_t R = final_pass ? g.final_rows : g.block_rows;
     const uint32_t nnodes = 1u << dn;
     const uint32_t maxn = (d.rows + nnodes - 1) >> dn;
     const uint32_t limit = final_pass ? d.rows_eval : maxn;
@@ -898,7 +904,7 @@ void build_task_passes(gf_ffa_program& P, TaskDev& d) {
       const uint32_t s0 = (u % bpn) * R;
       const uint32_t s1 = std::min<uint32_t>(s0 + R, final_pass ? d.rows_eval : X.n);
       if (s0 >= s1) continue;
-      build_column_block(d.bins, X.a, X.n, s0, s1, levels, P.max_rows, final_pass, P.col_meta, P.blocks);
+      build_column_block(d.bins, X.a, X.n, s0, s1, levels, g.max_rows, final_pass, P.col_meta, P.blocks);
     }
     pd.nblocks = static_cast<uint32_t>(P.blocks.size()) - pd.block_begin;
     P.passes.push_back(pd);
@@ -968,28 +974,37 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
       P->max_bins = std::max<uint32_t>(P->max_bins, static_cast<uint32_t>(t.bins));
     }
     for (uint64_t w : P->widths) P->max_width = std::max<uint32_t>(P->max_width, static_cast<uint32_t>(w));
-    // shared-memory geometry: two ColBlock headers, the staged schedule, two
-    // row buffers of max_rows rows; sized for two CTAs per SM
-    P->pitch = P->max_bins | 1u;
-    P->levels = 3;
+    // shared-memory geometry per NB: two ColBlock headers, the staged
+    // schedule, two row buffers of max_rows rows of the class's widest rows;
+    // sized for two CTAs per SM
     const size_t budget = 110 * 1024;
-    auto front_for = [&](uint32_t rows) {
-      const uint64_t meta_cap = std::max<uint64_t>(static_cast<uint64_t>(tree_depth(rows)) * rows,
-                                                   static_cast<uint64_t>(P->levels) * rows + 2);
-      return static_cast<uint32_t>(round_up(std::max<uint64_t>(32 + 2 * meta_cap, P->max_bins), 4));
-    };
-    auto smem_for = [&](uint32_t rows) { return (front_for(rows) + 2ull * rows * P->pitch) * 4; };
-    uint32_t rows = 8;
-    while (smem_for(rows + 1) <= budget) ++rows;
-    P->max_rows = rows;
-    P->front = front_for(rows);
-    // R + 3 (2^K - 1) rows at the bottom of a column
-    while (P->levels > 1 && static_cast<int>(rows) - 3 * ((1 << P->levels) - 1) < 8) --P->levels;
-    P->block_rows = rows - 3 * ((1u << P->levels) - 1);
-    const uint32_t cp_pitch = (P->max_bins + P->max_width + 2) | 1u;
-    P->final_rows = std::min<uint32_t>(P->block_rows, (rows * P->pitch) / cp_pitch);
-    check_arg(P->final_rows >= 1 && P->block_rows >= 1, "FFA bins too large for the shared-memory tiles");
-    P->smem_bytes = smem_for(rows);
+    uint32_t max_rows_all = 0;
+    for (uint32_t nb = 1; nb <= 16; ++nb) {
+      FfaGeometry& g = P->geo[nb];
+      const uint32_t cap = std::min<uint32_t>(32 * nb, P->max_bins);
+      if (32 * (nb - 1) >= P->max_bins) break;
+      g.pitch = cap | 1u;
+      g.levels = 3;
+      auto front_for = [&](uint32_t rows) {
+        const uint64_t meta_cap = std::max<uint64_t>(static_cast<uint64_t>(tree_depth(rows)) * rows,
+                                                     static_cast<uint64_t>(g.levels) * rows + 2);
+        return static_cast<uint32_t>(round_up(std::max<uint64_t>(32 + 2 * meta_cap, cap), 4));
+      };
+      auto smem_for = [&](uint32_t rows) { return (front_for(rows) + 2ull * rows * g.pitch) * 4; };
+      uint32_t rows = 8;
+      while (rows < 65535 && smem_for(rows + 1) <= budget) ++rows;
+      g.max_rows = rows;
+      g.front = front_for(rows);
+      // R + 3 (2^K - 1) rows at the bottom of a column
+      while (g.levels > 1 && static_cast<int>(rows) - 3 * ((1 << g.levels) - 1) < 8) --g.levels;
+      g.block_rows = rows - 3 * ((1u << g.levels) - 1);
+      const uint32_t cp_pitch = (cap + P->max_width + 2) | 1u;
+      g.final_rows = std::min<uint32_t>(g.block_rows, (rows * g.pitch) / cp_pitch);
+      check_arg(g.final_rows >= 1 && g.block_rows >= 1, "FFA bins too large for the shared-memory tiles");
+      g.smem_bytes = smem_for(rows);
+      max_rows_all = std::max(max_rows_all, rows);
+    }
+    const uint32_t rows = max_rows_all;
     // subtree schedules for every size up to max_rows
     P->sub_offset.assign(rows + 1, 0u);
     for (uint32_t n = 1; n <= rows; ++n) {
@@ -1020,11 +1035,13 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
         const float h = std::sqrt((bf - wf) / (bf * wf));
         P->trial_dev.push_back(TrialDev{h, wf / (bf - wf) * h, static_cast<uint32_t>(w), 0u});
       }
+      const uint32_t nbt = static_cast<uint32_t>(ceil_div(t.bins, 32));
+      const FfaGeometry& g = P->geo[nbt];
       uint32_t ds = 0;
-      while (ceil_div(t.rows, 1ull << ds) > rows) ++ds;
+      while (ceil_div(t.rows, 1ull << ds) > g.max_rows) ++ds;
       check_arg(ds <= 15, "FFA task too deep");
       d.split_depth = ds;
-      if (ds > 0) build_task_passes(*P, d);
+      if (ds > 0) build_task_passes(*P, g, d);
       P->task_dev.push_back(d);
       // cluster sized by rows for split tasks; on-chip tasks use key 0
       int cluster = 1;
@@ -1058,15 +1075,16 @@ extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, 
       std::stable_sort(c.tasks.begin(), c.tasks.end(), [&](uint32_t x, uint32_t y) {
         return P->tasks[x].rows * P->tasks[x].bins > P->tasks[y].rows * P->tasks[y].bins;
       });
+      const FfaGeometry& g = P->geo[c.nb];
       cuda_check(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(P->smem_bytes)),
+                                      static_cast<int>(g.smem_bytes)),
                  "cudaFuncSetAttribute(ffa_search_kernel)");
       cuda_check(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
                  "cudaFuncSetAttribute(cluster size)");
       cudaLaunchConfig_t cfg{};
       cfg.gridDim = dim3(c.cluster, 1, 1);
       cfg.blockDim = dim3(kThreads, 1, 1);
-      cfg.dynamicSmemBytes = P->smem_bytes;
+      cfg.dynamicSmemBytes = g.smem_bytes;
       cudaLaunchAttribute attr{};
       attr.id = cudaLaunchAttributeClusterDimension;
       attr.val.clusterDim.x = c.cluster;
@@ -1163,20 +1181,21 @@ extern "C" int gf_ffa_search(gf_ffa_program* P, const float* dev_prepared, uint6
     sp.col_meta = P->col_meta_d.as<MetaEntry>();
     sp.blocks = P->blocks_d.as<ColBlock>();
     sp.passes = P->passes_d.as<PassDev>();
-    sp.pitch = P->pitch;
-    sp.max_rows = P->max_rows;
-    sp.front = P->front;
     sp.scratch = static_cast<float*>(dev_scratch);
     for (const FfaClass& c : P->classes) {
       sp.item_tasks = c.tasks_d.as<uint32_t>();
       sp.nitem_tasks = static_cast<uint32_t>(c.tasks.size());
       sp.scratch_elems = c.max_elems;
+      const FfaGeometry& g = P->geo[c.nb];
+      sp.pitch = g.pitch;
+      sp.max_rows = g.max_rows;
+      sp.front = g.front;
       const uint64_t items = nseries * c.tasks.size();
       const unsigned nclusters = static_cast<unsigned>(std::min<uint64_t>(items, static_cast<uint64_t>(c.nclusters)));
       cudaLaunchConfig_t cfg{};
       cfg.gridDim = dim3(nclusters * c.cluster, 1, 1);
       cfg.blockDim = dim3(kThreads, 1, 1);
-      cfg.dynamicSmemBytes = P->smem_bytes;
+      cfg.dynamicSmemBytes = g.smem_bytes;
       cfg.stream = s;
       cudaLaunchAttribute attr{};
       attr.id = cudaLaunchAttributeClusterDimension;
