@@ -49,7 +49,8 @@ class DedispDesc(C.Structure):
                 ("dm_low", dbl), ("dm_step", dbl), ("ndm", u64), ("ref_frequency_mhz", dbl),
                 ("tsamp", dbl), ("chan_begin", u64), ("chan_end", u64), ("nbits", i32),
                 ("algorithm", i32), ("subband_channels", u64), ("ndm_per_nominal", u64),
-                ("device_id", i32), ("reserved", i32)]
+                ("device_id", i32), ("launch_dms_per_cta", i32), ("launch_chunk_rows", i32),
+                ("reserved", i32)]
 
 
 class DedispInfo(C.Structure):
@@ -71,6 +72,20 @@ class PreprocessInfo(C.Structure):
 class FfaInfo(C.Structure):
     _fields_ = [("ntasks", u64), ("noctaves", u64), ("prepared_floats", u64), ("scratch_bytes", u64),
                 ("max_task_elements", u64), ("metadata_bytes", u64), ("nclasses", u64)]
+
+
+class FfaBatchMember(C.Structure):
+    _fields_ = [("tasks", vp), ("ntasks", u64), ("widths", vp), ("nwidths", u64), ("nseries", u64)]
+
+
+class FfaMemberInfo(C.Structure):
+    _fields_ = [("nsamples", u64), ("nseries", u64), ("prepared_floats", u64), ("task_begin", u64),
+                ("ntasks", u64), ("noctaves", u64)]
+
+
+class DedispBatchItem(C.Structure):
+    _fields_ = [("program", vp), ("dev_staged", vp), ("dm_begin", u64), ("dm_count", u64), ("dev_out", vp),
+                ("out_stride", u64)]
 
 
 class CandidateOptions(C.Structure):
@@ -165,6 +180,15 @@ _SIGNATURES = [
     ("gf_ffa_search", C.c_int, [vp, vp, u64, C.c_float, vp, vp, u64, vp, vp]),
     ("gf_ffa_expand_peaks", C.c_int, [vp, vp, u64, u64, dbl, dbl, vp]),
     ("gf_ffa_transform", C.c_int, [vp, u64, u64, vp, vp, vp]),
+    ("gf_dedisp_batch_create", C.c_int, [C.POINTER(DedispBatchItem), u64, C.POINTER(vp)]),
+    ("gf_dedisp_batch_run", C.c_int, [vp, vp]),
+    ("gf_dedisp_batch_destroy", C.c_int, [vp]),
+    ("gf_ffa_batch_create", C.c_int, [C.POINTER(FfaBatchMember), u64, i32, C.POINTER(vp)]),
+    ("gf_ffa_batch_member_info", C.c_int, [vp, u64, C.POINTER(FfaMemberInfo)]),
+    ("gf_ffa_batch_bind", C.c_int, [vp, C.POINTER(vp)]),
+    ("gf_ffa_batch_prepare", C.c_int, [vp, u64, vp, u64, vp, vp]),
+    ("gf_ffa_batch_search", C.c_int, [vp, C.c_float, vp, vp, u64, vp, vp]),
+    ("gf_ffa_batch_expand_peaks", C.c_int, [vp, vp, u64, vp, vp, vp, vp, vp]),
     ("gf_sort_peaks", C.c_int, [vp, u64]),
     ("gf_select_candidates", C.c_int, [vp, u64, dbl, C.POINTER(CandidateOptions), vp, u64, C.POINTER(u64)]),
     ("gf_fold_workspace_bytes", u64, [u64, u64]),

@@ -115,6 +115,34 @@ def wide_subband(seed: int = 0, nsamples: int = 1 << 22, nchans: int = 4096,
         subband_channels=nchans // 64, ndm_per_nominal=int(math.ceil(20.0 / dm_step)))
 
 
+def batched_uneven(seed: int = 0, nobs: int = 64, nchans_choices=(1024, 2048, 4096), log2_nsamples=(20.0, 23.0),
+                   ndm_range=(256, 4096), dm_max: float = 1000.0, max_pulsars: int = 4) -> list:
+    """64 independent observations of uneven geometry: channels from
+    {1024, 2048, 4096} over 1200-1500 MHz, uint8, 64 us, lengths log-uniform
+    over 2^20-2^23 samples, 256-4096 DM trials over 0-dm_max, an FFA period
+    range drawn inside 0.1-10 s and 0-4 injected pulsars each (folded S/N
+    8-30, duty 1-5 %).  Observation i uses seed seed * 1000 + i.  The
+    keyword ranges give scaled-down batches of the same laws."""
+    tsamp = 64e-6
+    rng = np.random.default_rng(3_000_003 + seed)
+    out = []
+    for i in range(nobs):
+        nchans = int(rng.choice(nchans_choices))
+        nsamples = int(round(2.0 ** rng.uniform(*log2_nsamples) / 16.0)) * 16
+        ndm = int(rng.integers(ndm_range[0], ndm_range[1] + 1))
+        p_lo = float(math.exp(rng.uniform(math.log(0.1), math.log(1.0))))
+        p_hi = float(min(10.0, p_lo * math.exp(rng.uniform(math.log(2.0), math.log(100.0)))))
+        npsr = int(rng.integers(0, max_pulsars + 1))
+        obs = synth.Observation(
+            nchans=nchans, nsamples=nsamples, tsamp=tsamp, f_low=1200.0, f_high=1500.0, nbits=8,
+            seed=seed * 1000 + i,
+            pulsars=_survey_pulsars(rng, npsr, nchans, nsamples * tsamp, tsamp, dm_max, periods=(p_lo, p_hi)))
+        out.append(SearchConfig(
+            name=f"batched_uneven_{i}", obs=obs, dm_low=0.0, dm_step=dm_max / (ndm - 1), ndm=ndm,
+            period_min=p_lo, period_max=p_hi, duty_cycle_max=0.1))
+    return out
+
+
 CONFIGS = {
     "plain_end_to_end": plain_end_to_end,
     "survey_size": survey_size,

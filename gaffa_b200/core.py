@@ -93,9 +93,11 @@ class DedispersionProgram:
     def __init__(self, frequency_mhz, nsamples: int, tsamp: float, dm_low: float, dm_step: float,
                  ndm: int, ref_frequency_mhz: float | None = None, chan_begin: int = 0,
                  chan_end: int | None = None, nbits: int = 8, algorithm: str = "brute",
-                 subband_channels: int = 32, ndm_per_nominal: int = 32, device_id: int = 0):
+                 subband_channels: int = 32, ndm_per_nominal: int = 32, device_id: int = 0,
+                 launch_shape: tuple[int, int] | None = None):
         self.device = _require_cuda(device_id)
         self.device_id = device_id
+        self.launch_shape = launch_shape
         self.freq = np.ascontiguousarray(frequency_mhz, np.float64)
         nchans = len(self.freq)
         self.nbits = nbits
@@ -116,6 +118,9 @@ class DedispersionProgram:
         d.algorithm = {"brute": _lib.DEDISP_BRUTE, "subband": _lib.DEDISP_SUBBAND}[algorithm]
         d.subband_channels, d.ndm_per_nominal = subband_channels, ndm_per_nominal
         d.device_id = device_id
+        if launch_shape is not None:
+            # (DMs per CTA, channel rows per staging step); 0 = automatic
+            d.launch_dms_per_cta, d.launch_chunk_rows = launch_shape
         h = C.c_void_p()
         with torch.cuda.device(self.device):
             check(_lib.lib().gf_dedisp_program_create(C.byref(d), C.byref(h)))
@@ -146,10 +151,16 @@ class DedispersionProgram:
         check(_lib.lib().gf_dedisp_workspace_bytes(self._h, dm_count, C.byref(b)))
         return int(b.value)
 
-    def stage(self, data, stream=None) -> torch.Tensor:
+    def stage(self, data, stream=None, out: torch.Tensor | None = None) -> torch.Tensor:
         """Channel-major staging of a time-major input (device tensor, or host
-        numpy array / tensor copied through a bounce buffer)."""
-        staged = torch.empty(int(self.info.staged_bytes), dtype=torch.uint8, device=self.device)
+        numpy array / tensor copied through a bounce buffer), into `out` when
+        given (uint8, at least staged_bytes)."""
+        if out is None:
+            staged = torch.empty(int(self.info.staged_bytes), dtype=torch.uint8, device=self.device)
+        else:
+            if out.dtype != torch.uint8 or out.numel() < self.info.staged_bytes or out.device != self.device:
+                raise ValueError("staging buffer must be uint8 on the program's device with staged_bytes bytes")
+            staged = out
         with torch.cuda.device(self.device):
             if isinstance(data, torch.Tensor) and data.is_cuda:
                 if data.numel() * data.element_size() != self.info.input_bytes:
@@ -183,6 +194,49 @@ class DedispersionProgram:
             check(_lib.lib().gf_dedisp_run(self._h, ptr(staged), dm_begin, dm_count, ptr(out), out_stride,
                                            ptr(workspace), _stream(stream)))
         return out.view(-1)[: dm_count * out_stride].view(dm_count, out_stride)
+
+
+class DedispersionBatch:
+    """Many brute-force (program, staged input, DM range, output) items of
+    different observations as one kernel launch (gf_dedisp_batch_*).  Device
+    pointers are fixed here, so run() can be captured in a CUDA graph; the
+    tensors must stay alive as long as the batch."""
+
+    def __init__(self, items):
+        items = list(items)
+        if not items:
+            raise ValueError("batched dedispersion needs at least one item")
+        arr = (_lib.DedispBatchItem * len(items))()
+        self._keep = []
+        device = None
+        for i, (program, staged, dm_begin, dm_count, out, out_stride) in enumerate(items):
+            if program.algorithm != "brute":
+                raise ValueError("batched dedispersion takes brute-force programs")
+            if out.numel() < dm_count * out_stride:
+                raise ValueError("output too small for the DM range")
+            arr[i].program = program._h
+            arr[i].dev_staged = ptr(staged)
+            arr[i].dm_begin, arr[i].dm_count = dm_begin, dm_count
+            arr[i].dev_out = ptr(out)
+            arr[i].out_stride = out_stride
+            self._keep += [program, staged, out]
+            device = program.device
+        self.device = device
+        h = C.c_void_p()
+        with torch.cuda.device(device):
+            check(_lib.lib().gf_dedisp_batch_create(arr, len(items), C.byref(h)))
+        self._h = h
+
+    def run(self, stream=None) -> None:
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_dedisp_batch_run(self._h, _stream(stream)))
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.gf_dedisp_batch_destroy(h)
+
+    __del__ = close
 
 
 # ---------------------------------------------------------------------------
@@ -331,6 +385,125 @@ class FfaProgram:
         check(_lib.lib().gf_ffa_expand_peaks(self._h, ptr(records), len(records), series_offset, dm_low, dm_step,
                                              ptr(out)))
         return out
+
+
+class FfaBatchProgram:
+    """The FFA plans of many observations (members) as one program
+    (gf_ffa_batch_*): one persistent launch per class searches every member's
+    series.  members: [(FfaPlan, nseries)].  The prepared buffers are bound
+    once, so prepare() and search_async() can be captured in a CUDA graph."""
+
+    def __init__(self, members, device_id: int = 0, prepared=None, scratch=None):
+        """prepared (optional): one float32 [nseries][prepared_floats] buffer
+        per member (views of a shared arena, say); scratch (optional): a
+        uint8 buffer of at least scratch_bytes, or False to attach one later
+        with use_scratch (programs that run one after another share one)."""
+        self.device = _require_cuda(device_id)
+        members = list(members)
+        if not members:
+            raise ValueError("a batched FFA program needs at least one member")
+        self.plans = [m[0] for m in members]
+        self.nseries = [int(m[1]) for m in members]
+        arr = (_lib.FfaBatchMember * len(members))()
+        self._keep = []
+        for i, (plan, nseries) in enumerate(members):
+            widths = np.ascontiguousarray(plan.width_trials, np.uint64)
+            tasks = np.ascontiguousarray(plan.tasks)
+            self._keep += [widths, tasks]
+            arr[i].tasks, arr[i].ntasks = tasks.ctypes.data, len(tasks)
+            arr[i].widths, arr[i].nwidths = widths.ctypes.data, len(widths)
+            arr[i].nseries = nseries
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_ffa_batch_create(arr, len(members), device_id, C.byref(h)))
+        self._h = h
+        self.info = _lib.FfaInfo()
+        check(_lib.lib().gf_ffa_program_info(h, C.byref(self.info)))
+        self.member_info = []
+        for i in range(len(members)):
+            mi = _lib.FfaMemberInfo()
+            check(_lib.lib().gf_ffa_batch_member_info(h, i, C.byref(mi)))
+            self.member_info.append(mi)
+        if prepared is None:
+            prepared = [torch.empty((int(mi.nseries), int(mi.prepared_floats)), dtype=torch.float32,
+                                    device=self.device) for mi in self.member_info]
+        for t, mi in zip(prepared, self.member_info):
+            if t.dtype != torch.float32 or t.numel() < mi.nseries * mi.prepared_floats:
+                raise ValueError("prepared buffer too small for its member")
+        self.prepared = list(prepared)
+        ptrs = (C.c_void_p * len(members))(*[t.data_ptr() for t in self.prepared])
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_ffa_batch_bind(h, ptrs))
+        self.scratch = None
+        if scratch is None:
+            scratch = torch.empty(max(16, int(self.info.scratch_bytes)), dtype=torch.uint8, device=self.device)
+        if scratch is not False:
+            self.use_scratch(scratch)
+        self.counters = torch.zeros(2, dtype=torch.int64, device=self.device)
+        self.capacity = 1 << 16
+        self.peaks = torch.empty(self.capacity * 24, dtype=torch.uint8, device=self.device)
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.gf_ffa_program_destroy(h)
+
+    __del__ = close
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.info.nclasses)
+
+    @property
+    def scratch_bytes(self) -> int:
+        return int(self.info.scratch_bytes)
+
+    def use_scratch(self, scratch: torch.Tensor) -> None:
+        """Search scratch (programs that run one after another may share one)."""
+        if scratch.numel() * scratch.element_size() < self.info.scratch_bytes:
+            raise ValueError("FFA scratch too small")
+        self.scratch = scratch
+
+    def prepare(self, member: int, series: torch.Tensor, stats: torch.Tensor, stream=None) -> None:
+        """prepare_ffa_input_cuda of the member's nseries rows of series."""
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_ffa_batch_prepare(self._h, member, ptr(series), series.stride(0), ptr(stats),
+                                                  _stream(stream)))
+
+    def search_async(self, snr_threshold: float, stream=None) -> None:
+        if self.scratch is None:
+            raise RuntimeError("batched FFA program has no scratch: call use_scratch")
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_ffa_batch_search(self._h, snr_threshold, ptr(self.scratch), ptr(self.peaks),
+                                                 self.capacity, ptr(self.counters), _stream(stream)))
+
+    def collect(self, snr_threshold: float, rerun=None) -> np.ndarray:
+        """Records of the last search; on a peak-buffer overflow grows the
+        buffer and calls rerun() (default: search_async again)."""
+        while True:
+            counts = self.counters.cpu()
+            if int(counts[1]) & _lib.STATUS_SCHEDULE:
+                raise RuntimeError("FFA block schedule exceeded its shared-memory tile")
+            n = int(counts[0])
+            if n <= self.capacity:
+                break
+            self.capacity = int(n * 1.25) + 1024
+            self.peaks = torch.empty(self.capacity * 24, dtype=torch.uint8, device=self.device)
+            (rerun or (lambda: self.search_async(snr_threshold)))()
+        raw = self.peaks[: n * 24].cpu().numpy()
+        return raw.view(_lib.PEAK_RECORD_DTYPE).copy()
+
+    def expand(self, records: np.ndarray, series_offset, dm_low, dm_step) -> tuple[np.ndarray, np.ndarray]:
+        """(peaks, member of each peak); series_offset / dm_low / dm_step per member."""
+        records = np.ascontiguousarray(records, _lib.PEAK_RECORD_DTYPE)
+        out = np.zeros(len(records), _lib.PEAK_DTYPE)
+        member = np.zeros(len(records), np.uint32)
+        so = np.ascontiguousarray(series_offset, np.uint64)
+        lo = np.ascontiguousarray(dm_low, np.float64)
+        st = np.ascontiguousarray(dm_step, np.float64)
+        check(_lib.lib().gf_ffa_batch_expand_peaks(self._h, ptr(records), len(records), ptr(so), ptr(lo), ptr(st),
+                                                   ptr(out), ptr(member)))
+        return out, member
 
 
 def ffa_transform(x: torch.Tensor, bins: int, stream=None) -> torch.Tensor:

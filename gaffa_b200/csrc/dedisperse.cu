@@ -86,6 +86,8 @@ struct BytesParams {
   uint64_t out_dm_rows;
   uint64_t out_group_rows;
   uint64_t nout;             // valid output samples
+  uint32_t grid_x;           // CTAs per group (grid x)
+  uint32_t reserved;
 };
 
 __device__ __forceinline__ uint32_t lo16(uint32_t v) { return v & 0xffffu; }
@@ -153,13 +155,12 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// One CTA of a bytes launch: CTA bx of group `group` (grid x and z).
 template <typename OutT>
-__global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesParams p) {
-  extern __shared__ __align__(16) uint8_t smem[];
-  const int group = blockIdx.z;
+__device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int group, uint8_t* smem) {
   // DM block fastest: the CTAs resident at once share their input windows in L2
-  const int block = static_cast<int>(blockIdx.x % static_cast<unsigned>(p.nblocks));
-  const uint64_t t0 = static_cast<uint64_t>(blockIdx.x / static_cast<unsigned>(p.nblocks)) * p.cta_samples;
+  const int block = static_cast<int>(bx % static_cast<unsigned>(p.nblocks));
+  const uint64_t t0 = static_cast<uint64_t>(bx / static_cast<unsigned>(p.nblocks)) * p.cta_samples;
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int dm_sub = warp / p.warps_per_dm;
@@ -284,6 +285,35 @@ __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesPara
         if (t + q < p.nout) out[t + q] = static_cast<OutT>(acc[m][q]);
     }
   }
+}
+
+template <typename OutT>
+__global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesParams p) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  bytes_cta<OutT>(p, blockIdx.x, static_cast<int>(blockIdx.z), smem);
+}
+
+// Many launches (programs, DM ranges, observations) as one grid: CTA b runs
+// CTA b - block_begin[i] of launch i, the last launch starting at or before b.
+__global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_batch_kernel(const BytesParams* __restrict__ items,
+                                                                             const uint64_t* __restrict__ block_begin,
+                                                                             int nitems) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ BytesParams sp;
+  __shared__ uint32_t s_local;
+  if (threadIdx.x == 0) {
+    const uint64_t b = blockIdx.x;
+    int lo = 0, hi = nitems;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (block_begin[mid] <= b) lo = mid; else hi = mid;
+    }
+    sp = items[lo];
+    s_local = static_cast<uint32_t>(b - block_begin[lo]);
+  }
+  __syncthreads();
+  const uint32_t local = s_local;
+  bytes_cta<uint32_t>(sp, local % sp.grid_x, static_cast<int>(local / sp.grid_x), smem);
 }
 
 // Stage-2 sum over uint32 intermediate rows (subband with 8-bit input, where
@@ -436,15 +466,19 @@ struct Launch {
 
 // Picks the DM block size and channel chunk so the staged windows fit in
 // shared memory with two CTAs per SM when possible.
+// dpc_fix / cr_fix (0 = any) pin the DM block or the chunk rows (launch
+// shapes picked by an autotuner); every shape gives the same sums.
 template <typename F>
-Launch choose_launch(F&& max_off_for) {
+Launch choose_launch(F&& max_off_for, int dpc_fix, int cr_fix) {
   const size_t budget2 = 110 * 1024, budget1 = 220 * 1024;
   for (size_t budget : {budget2, budget1}) {
     for (int dpc : {8, 4, 2, 1}) {
+      if (dpc_fix && dpc != dpc_fix) continue;
       const int wpd = kWarps / dpc;
       const int max_off = max_off_for(dpc);
       const int row_bytes = static_cast<int>(round_up(max_off + 4 * ((wpd - 1) * kOutWords + 32 * kWords), 16));
       for (int cr : {64, 32, 16, 8}) {
+        if (cr_fix && cr != cr_fix) continue;
         const size_t rec = static_cast<size_t>(dpc) * round_up(1 + (cr + 4) / 2, 4) * 4;
         const size_t smem = 2 * (static_cast<size_t>(cr + 1) * row_bytes + rec);  // double-buffered
         if (smem <= budget && static_cast<size_t>(cr + 1) * row_bytes < 262144) {
@@ -481,12 +515,14 @@ struct BytesStage {
   DeviceBlob base_dev, rec_dev;
   int ngroups = 0, ndm_group = 0, rows_per_group = 0, total_rows = 0, blocks = 0;
 
-  void build(const std::vector<int32_t>& delays, int ng, int ndg, int rpg, int tr, int device) {
+  void build(const std::vector<int32_t>& delays, int ng, int ndg, int rpg, int tr, int device, int dpc_fix = 0,
+             int cr_fix = 0) {
     ngroups = ng;
     ndm_group = ndg;
     rows_per_group = rpg;
     total_rows = tr;
-    launch = choose_launch([&](int dpc) { return max_off_estimate(delays, ng, ndg, rpg, tr, dpc); });
+    launch = choose_launch([&](int dpc) { return max_off_estimate(delays, ng, ndg, rpg, tr, dpc); }, dpc_fix,
+                           cr_fix);
     blocks = static_cast<int>(ceil_div(ndg, launch.dms_per_cta));
     rec = build_records(delays, ng, ndg, rpg, tr, launch.dms_per_cta, launch.chunk_rows, launch.row_bytes);
     base_dev.upload(rec.base.data(), rec.base.size() * sizeof(int32_t), device);
@@ -499,11 +535,10 @@ struct BytesStage {
   // [dm_first, dm_first + dm_count) (dm_first a multiple of the DM block);
   // the last launched group handles dm_count_last DMs.  in / out point at the
   // launch's first group and first output row.
-  template <typename OutT>
-  void run(const uint8_t* in, uint64_t row_stride, uint64_t group_stride, uint64_t valid, int g0,
-           int gcount, int dm_first, int dm_count, int dm_count_last, void* out,
-           uint64_t out_row_stride, uint64_t out_dm_rows, uint64_t out_group_rows, uint64_t nout,
-           cudaStream_t stream) const {
+  BytesParams params(const uint8_t* in, uint64_t row_stride, uint64_t group_stride, uint64_t valid, int g0,
+                     int gcount, int dm_first, int dm_count, int dm_count_last, void* out,
+                     uint64_t out_row_stride, uint64_t out_dm_rows, uint64_t out_group_rows,
+                     uint64_t nout) const {
     if (dm_first % launch.dms_per_cta != 0) raise(GF_EINVAL, "DM range not aligned to the DM block");
     BytesParams p{};
     p.in = in;
@@ -538,7 +573,18 @@ struct BytesStage {
     p.one = 1u;
     const uint64_t ctas = ceil_div(nout, p.cta_samples) * static_cast<uint64_t>(p.nblocks);
     if (ctas >= (1ull << 31)) raise(GF_EINVAL, "dedispersion launch too large");
-    dim3 grid(static_cast<unsigned>(ctas), 1u, static_cast<unsigned>(gcount));
+    p.grid_x = static_cast<uint32_t>(ctas);
+    return p;
+  }
+
+  template <typename OutT>
+  void run(const uint8_t* in, uint64_t row_stride, uint64_t group_stride, uint64_t valid, int g0,
+           int gcount, int dm_first, int dm_count, int dm_count_last, void* out,
+           uint64_t out_row_stride, uint64_t out_dm_rows, uint64_t out_group_rows, uint64_t nout,
+           cudaStream_t stream) const {
+    const BytesParams p = params(in, row_stride, group_stride, valid, g0, gcount, dm_first, dm_count,
+                                 dm_count_last, out, out_row_stride, out_dm_rows, out_group_rows, nout);
+    dim3 grid(p.grid_x, 1u, static_cast<unsigned>(gcount));
     auto kernel = dedisperse_bytes_kernel<OutT>;
     cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(launch.smem)),
@@ -601,6 +647,12 @@ void validate_desc(const gf_dedisp_desc& d) {
     check_arg(d.ndm_per_nominal > 0, "ndm_per_nominal must be positive");
   }
   check_arg(d.chan_end - d.chan_begin < 65536, "at most 65535 channels per program");
+  check_arg(d.launch_dms_per_cta == 0 || d.launch_dms_per_cta == 1 || d.launch_dms_per_cta == 2 ||
+                d.launch_dms_per_cta == 4 || d.launch_dms_per_cta == 8,
+            "launch_dms_per_cta must be 0, 1, 2, 4 or 8");
+  check_arg(d.launch_chunk_rows == 0 || d.launch_chunk_rows == 8 || d.launch_chunk_rows == 16 ||
+                d.launch_chunk_rows == 32 || d.launch_chunk_rows == 64,
+            "launch_chunk_rows must be 0, 8, 16, 32 or 64");
   check_arg(d.ndm < (1ull << 31), "too many DM trials");
 }
 
@@ -636,7 +688,8 @@ extern "C" int gf_dedisp_program_create(const gf_dedisp_desc* desc, gf_dedisp_pr
         for (uint64_t c = 0; c < P.nc; ++c)
           delays[dm * P.nc + c] = delay_bins(v, P.freq[d.chan_begin + c], d.ref_frequency_mhz, d.tsamp);
       }
-      P.brute.build(delays, 1, static_cast<int>(d.ndm), nc, nc, d.device_id);
+      P.brute.build(delays, 1, static_cast<int>(d.ndm), nc, nc, d.device_id, d.launch_dms_per_cta,
+                    d.launch_chunk_rows);
     } else {
       // dedispersion.cpp:360-388 subband geometry and tables
       P.sbc = d.subband_channels;
@@ -837,6 +890,71 @@ extern "C" int gf_dedisp_workspace_bytes(const gf_dedisp_program* P, uint64_t dm
     const uint64_t groups = std::min<uint64_t>(ceil_div(dm_count, P->npn) + 2 * dpc1, P->nnom + dpc1);
     *bytes = groups * P->nsb * P->inter_row_stride * (P->inter_u8 ? 1 : 4);
   });
+}
+
+// Batched brute-force dedispersion: the launches of many (program, DM range)
+// items as one grid of dedisperse_bytes_batch_kernel.
+struct gf_dedisp_batch {
+  int device = 0;
+  int nitems = 0;
+  uint64_t blocks = 0;
+  size_t smem = 0;
+  DeviceBlob items_d, begin_d;
+};
+
+extern "C" int gf_dedisp_batch_create(const gf_dedisp_batch_item* items, uint64_t nitems, gf_dedisp_batch** out) {
+  return guarded([&] {
+    check_arg(items && out, "null argument");
+    *out = nullptr;
+    check_arg(nitems > 0 && nitems < (1u << 20), "batched dedispersion takes 1 to 2^20 items");
+    auto B = std::make_unique<gf_dedisp_batch>();
+    std::vector<BytesParams> params;
+    std::vector<uint64_t> begin;
+    for (uint64_t i = 0; i < nitems; ++i) {
+      const gf_dedisp_batch_item& it = items[i];
+      check_arg(it.program && it.dev_staged && it.dev_out, "null argument");
+      const gf_dedisp_program* P = it.program;
+      const auto& d = P->desc;
+      check_arg(d.algorithm == GF_DEDISP_BRUTE, "batched dedispersion takes brute-force programs");
+      check_arg(i == 0 || d.device_id == B->device, "batched dedispersion items must share one device");
+      B->device = d.device_id;
+      check_arg(it.dm_count > 0 && it.dm_begin < d.ndm && it.dm_begin + it.dm_count <= d.ndm,
+                "DM range out of bounds");
+      check_arg(it.dm_begin % 8 == 0, "dm_begin must be a multiple of 8");
+      check_arg(it.out_stride >= P->nout, "out_stride must be >= nout");
+      const BytesParams bp = P->brute.params(static_cast<const uint8_t*>(it.dev_staged), P->row_stride, 0,
+                                             d.nsamples, 0, 1, static_cast<int>(it.dm_begin),
+                                             static_cast<int>(it.dm_count), static_cast<int>(it.dm_count),
+                                             it.dev_out, it.out_stride, 1, 0, P->nout);
+      begin.push_back(B->blocks);
+      B->blocks += bp.grid_x;
+      B->smem = std::max(B->smem, P->brute.launch.smem);
+      params.push_back(bp);
+    }
+    check_arg(B->blocks < (1ull << 31), "batched dedispersion launch too large");
+    B->nitems = static_cast<int>(nitems);
+    DeviceGuard dg(B->device);
+    B->items_d.upload(params.data(), params.size() * sizeof(BytesParams), B->device);
+    B->begin_d.upload(begin.data(), begin.size() * sizeof(uint64_t), B->device);
+    *out = B.release();
+  });
+}
+
+extern "C" int gf_dedisp_batch_run(gf_dedisp_batch* B, void* stream) {
+  return guarded([&] {
+    check_arg(B != nullptr, "null argument");
+    DeviceGuard dg(B->device);
+    cuda_check(cudaFuncSetAttribute(dedisperse_bytes_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(B->smem)),
+               "cudaFuncSetAttribute(dedisperse batch smem)");
+    dedisperse_bytes_batch_kernel<<<static_cast<unsigned>(B->blocks), kThreads, B->smem, as_stream(stream)>>>(
+        B->items_d.as<BytesParams>(), B->begin_d.as<uint64_t>(), B->nitems);
+    cuda_check(cudaGetLastError(), "dedisperse_bytes_batch_kernel launch");
+  });
+}
+
+extern "C" int gf_dedisp_batch_destroy(gf_dedisp_batch* B) {
+  return guarded([&] { delete B; });
 }
 
 extern "C" int gf_dedisperse_spectrum(const void* dev_in, int32_t elem_bytes, uint64_t nsamples, uint64_t nchans,

@@ -56,7 +56,20 @@ struct TaskDev {
   uint32_t max_width;
   uint32_t pass_begin;    // column passes (split_depth > 0)
   uint32_t npasses;
-  uint32_t reserved;
+  uint32_t member;        // observation of a batched program (0 otherwise)
+};
+
+// Batched programs: one observation's prepared series, and a run of items
+// (all series of one task of one observation) in a class's item order.
+struct MemberDev {
+  const float* prepared;
+  uint64_t prep_stride;
+};
+
+struct UnitDev {
+  uint64_t item_begin;
+  uint32_t task;
+  uint32_t member;
 };
 
 struct TrialDev {
@@ -450,6 +463,10 @@ struct SearchParams {
   const uint32_t* item_tasks;   // task indices of this launch's class
   uint32_t nitem_tasks;
   uint32_t nseries;
+  const UnitDev* units;         // batched programs: item runs of this class (else null)
+  const MemberDev* members;
+  uint32_t nunits;
+  uint64_t nitems;
   float threshold;
   gf_peak_record* peaks;
   uint64_t capacity;
@@ -562,12 +579,31 @@ __global__ void __launch_bounds__(kThreads, 2) ffa_search_kernel(SearchParams p)
   float* buf1 = buf0 + p.max_rows * pitch;
   float* q0 = p.scratch ? p.scratch + static_cast<uint64_t>(cid) * 2 * p.scratch_elems : nullptr;
   float* q1 = q0 ? q0 + p.scratch_elems : nullptr;
-  const uint64_t nitems = static_cast<uint64_t>(p.nseries) * p.nitem_tasks;
+  const uint64_t nitems = p.units ? p.nitems : static_cast<uint64_t>(p.nseries) * p.nitem_tasks;
   for (uint64_t item = cid; item < nitems; item += nclusters) {
-    const uint32_t task = p.item_tasks[item / p.nseries];
-    const uint32_t series = static_cast<uint32_t>(item % p.nseries);
+    uint32_t task, series;
+    const float* base;
+    uint64_t stride;
+    if (p.units) {
+      // last run starting at or before the item (runs in item order)
+      uint32_t lo = 0, hi = p.nunits;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (p.units[mid].item_begin <= item) lo = mid; else hi = mid;
+      }
+      const UnitDev u = p.units[lo];
+      task = u.task;
+      series = static_cast<uint32_t>(item - u.item_begin);
+      base = p.members[u.member].prepared;
+      stride = p.members[u.member].prep_stride;
+    } else {
+      task = p.item_tasks[item / p.nseries];
+      series = static_cast<uint32_t>(item % p.nseries);
+      base = p.prepared;
+      stride = p.prep_stride;
+    }
     const TaskDev t = p.tasks[task];
-    const float* input = p.prepared + series * p.prep_stride + t.prep_offset;
+    const float* input = base + series * stride + t.prep_offset;
     const uint32_t bins = t.bins;
     const DetectArgs da = make_detect(p, t, series, task);
     const uint32_t cp_pitch = (bins + t.max_width + 2) | 1u;
@@ -692,29 +728,44 @@ struct FfaClass {
   uint64_t max_elems = 0;      // rows * bins of the largest task (scratch per cluster)
   int nclusters = 0;           // resident clusters
   DeviceBlob tasks_d;
+  std::vector<UnitDev> units;  // batched programs: one item run per task, in task order
+  uint64_t nitems = 0;
+  DeviceBlob units_d;
+};
+
+// One observation's plan inside a program; a single-plan program has one.
+struct FfaMember {
+  uint64_t nsamples = 0;
+  uint64_t prep_stride = 0;    // prepared floats per series (all octaves)
+  uint64_t halo = 0;
+  uint64_t nseries = 0;        // series per search (batched programs)
+  uint32_t task_begin = 0, ntasks = 0, max_width = 0;
+  std::vector<uint64_t> widths;
+  std::vector<OctaveDev> octaves;
+  DeviceBlob octaves_d;
+  const float* prepared = nullptr;  // bound prepared series (batched programs)
 };
 
 struct gf_ffa_program {
   int device = 0;
-  std::vector<gf_ffa_task> tasks;
-  std::vector<uint64_t> widths;
+  bool batched = false;
+  bool bound = false;
+  std::vector<gf_ffa_task> tasks;        // every member's tasks, member by member
+  std::vector<uint32_t> task_member;
+  std::vector<FfaMember> members;
   std::vector<TaskDev> task_dev;
   std::vector<TrialDev> trial_dev;
-  std::vector<OctaveDev> octaves;
   std::vector<MetaEntry> sub_meta;
   std::vector<uint32_t> sub_offset;
   std::vector<MetaEntry> col_meta;
   std::vector<ColBlock> blocks;
   std::vector<PassDev> passes;
   std::vector<FfaClass> classes;
-  uint64_t nsamples = 0;
-  uint64_t prep_stride = 0;
   uint32_t max_bins = 0, max_width = 0;
   FfaGeometry geo[17];         // by NB (1..16)
-  uint64_t halo = 0;
   uint64_t max_series = 0;
   uint64_t scratch_floats = 0;
-  DeviceBlob tasks_d, trials_d, octaves_d, sub_meta_d, sub_offset_d, col_meta_d, blocks_d, passes_d;
+  DeviceBlob tasks_d, trials_d, sub_meta_d, sub_offset_d, col_meta_d, blocks_d, passes_d, members_d;
 };
 
 namespace {
@@ -937,178 +988,347 @@ extern "C" int gf_ffa_task_stdnoise(const gf_ffa_task* t, float* out) {
   });
 }
 
-extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, const uint64_t* widths,
-                                     uint64_t nwidths, uint64_t max_series, int32_t device_id,
-                                     gf_ffa_program** out) {
-  return guarded([&] {
-    check_arg(tasks && widths && out, "null argument");
-    *out = nullptr;
-    check_arg(ntasks > 0, "FFA executor plan must contain at least one task");
-    check_arg(nwidths > 0, "FFA search plan width_trials must not be empty");
-    check_arg(nwidths <= kMaxWidths, "at most 64 width trials");
-    check_arg(max_series > 0 && max_series < (1ull << 31), "max_series out of range");
-    DeviceGuard dg(device_id);
-    auto P = std::make_unique<gf_ffa_program>();
-    P->device = device_id;
-    P->tasks.assign(tasks, tasks + ntasks);
-    P->widths.assign(widths, widths + nwidths);
-    P->max_series = max_series;
-    P->nsamples = tasks[0].input_nsamples;
-    for (const auto& t : P->tasks) validate_task(t, P->nsamples);
+namespace {
+
+struct MemberSpec {
+  const gf_ffa_task* tasks;
+  uint64_t ntasks;
+  const uint64_t* widths;
+  uint64_t nwidths;
+  uint64_t nseries;
+};
+
+// Tables of every member's tasks: octaves, boxcar trials, on-chip geometry,
+// column schedules and the launch classes.  Batched programs also get one
+// item run per (task, member) so one launch per class covers every member.
+std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& specs, bool batched,
+                                              uint64_t max_series, int device_id) {
+  auto P = std::make_unique<gf_ffa_program>();
+  P->device = device_id;
+  P->batched = batched;
+  P->max_series = max_series;
+  std::vector<std::map<double, uint32_t>> octave_of(specs.size());
+  for (size_t m = 0; m < specs.size(); ++m) {
+    const MemberSpec& s = specs[m];
+    check_arg(s.tasks && s.widths, "null argument");
+    check_arg(s.ntasks > 0, "FFA executor plan must contain at least one task");
+    check_arg(s.nwidths > 0, "FFA search plan width_trials must not be empty");
+    check_arg(s.nwidths <= kMaxWidths, "at most 64 width trials");
+    check_arg(P->tasks.size() + s.ntasks < (1ull << 31), "too many FFA tasks");
+    FfaMember M;
+    M.nsamples = s.tasks[0].input_nsamples;
+    M.nseries = s.nseries;
+    M.task_begin = static_cast<uint32_t>(P->tasks.size());
+    M.ntasks = static_cast<uint32_t>(s.ntasks);
+    M.widths.assign(s.widths, s.widths + s.nwidths);
+    for (uint64_t i = 0; i < s.ntasks; ++i) validate_task(s.tasks[i], M.nsamples);
     // octaves = distinct prepare keys in plan order
-    std::map<double, uint32_t> octave_of;
     uint64_t off = 0;
-    for (const auto& t : P->tasks) {
-      if (octave_of.count(t.downsample_factor)) continue;
-      octave_of[t.downsample_factor] = static_cast<uint32_t>(P->octaves.size());
-      OctaveDev o{t.downsample_factor, t.prepared_nsamples, off};
-      P->octaves.push_back(o);
+    for (uint64_t i = 0; i < s.ntasks; ++i) {
+      const gf_ffa_task& t = s.tasks[i];
+      if (octave_of[m].count(t.downsample_factor)) continue;
+      octave_of[m][t.downsample_factor] = static_cast<uint32_t>(M.octaves.size());
+      M.octaves.push_back(OctaveDev{t.downsample_factor, t.prepared_nsamples, off});
       off = round_up(off + t.prepared_nsamples, 4);
-      P->halo = std::max<uint64_t>(P->halo, static_cast<uint64_t>(std::ceil(t.downsample_factor)) + 2);
+      M.halo = std::max<uint64_t>(M.halo, static_cast<uint64_t>(std::ceil(t.downsample_factor)) + 2);
     }
-    check_arg(P->octaves.size() <= 32, "at most 32 distinct downsample factors");
-    P->prep_stride = round_up(off, 4);
-    for (const auto& t : P->tasks) {
+    check_arg(M.octaves.size() <= 32, "at most 32 distinct downsample factors");
+    M.prep_stride = round_up(off, 4);
+    for (uint64_t i = 0; i < s.ntasks; ++i) {
+      const gf_ffa_task& t = s.tasks[i];
       check_arg(t.bins <= kMaxBins, "FFA CUDA path supports bins <= 512");
       check_arg(t.rows < 65536, "FFA CUDA path supports at most 65535 rows per task");
       P->max_bins = std::max<uint32_t>(P->max_bins, static_cast<uint32_t>(t.bins));
     }
-    for (uint64_t w : P->widths) P->max_width = std::max<uint32_t>(P->max_width, static_cast<uint32_t>(w));
-    // shared-memory geometry per NB: two ColBlock headers, the staged
-    // schedule, two row buffers of max_rows rows of the class's widest rows;
-    // sized for two CTAs per SM
-    const size_t budget = 110 * 1024;
-    uint32_t max_rows_all = 0;
-    for (uint32_t nb = 1; nb <= 16; ++nb) {
-      FfaGeometry& g = P->geo[nb];
-      const uint32_t cap = std::min<uint32_t>(32 * nb, P->max_bins);
-      if (32 * (nb - 1) >= P->max_bins) break;
-      g.pitch = cap | 1u;
-      g.levels = 3;
-      auto front_for = [&](uint32_t rows) {
-        const uint64_t meta_cap = std::max<uint64_t>(static_cast<uint64_t>(tree_depth(rows)) * rows,
-                                                     static_cast<uint64_t>(g.levels) * rows + 2);
-        return static_cast<uint32_t>(round_up(std::max<uint64_t>(32 + 2 * meta_cap, cap), 4));
-      };
-      auto smem_for = [&](uint32_t rows) { return (front_for(rows) + 2ull * rows * g.pitch) * 4; };
-      uint32_t rows = 8;
-      while (rows < 65535 && smem_for(rows + 1) <= budget) ++rows;
-      g.max_rows = rows;
-      g.front = front_for(rows);
-      // R + 3 (2^K - 1) rows at the bottom of a column
-      while (g.levels > 1 && static_cast<int>(rows) - 3 * ((1 << g.levels) - 1) < 8) --g.levels;
-      g.block_rows = rows - 3 * ((1u << g.levels) - 1);
-      const uint32_t cp_pitch = (cap + P->max_width + 2) | 1u;
-      g.final_rows = std::min<uint32_t>(g.block_rows, (rows * g.pitch) / cp_pitch);
-      check_arg(g.final_rows >= 1 && g.block_rows >= 1, "FFA bins too large for the shared-memory tiles");
-      g.smem_bytes = smem_for(rows);
-      max_rows_all = std::max(max_rows_all, rows);
+    for (uint64_t w : M.widths) M.max_width = std::max<uint32_t>(M.max_width, static_cast<uint32_t>(w));
+    P->max_width = std::max(P->max_width, M.max_width);
+    P->tasks.insert(P->tasks.end(), s.tasks, s.tasks + s.ntasks);
+    P->task_member.insert(P->task_member.end(), s.ntasks, static_cast<uint32_t>(m));
+    P->members.push_back(std::move(M));
+  }
+  // shared-memory geometry per NB: two ColBlock headers, the staged
+  // schedule, two row buffers of max_rows rows of the class's widest rows;
+  // sized for two CTAs per SM
+  const size_t budget = 110 * 1024;
+  uint32_t max_rows_all = 0;
+  for (uint32_t nb = 1; nb <= 16; ++nb) {
+    FfaGeometry& g = P->geo[nb];
+    const uint32_t cap = std::min<uint32_t>(32 * nb, P->max_bins);
+    if (32 * (nb - 1) >= P->max_bins) break;
+    g.pitch = cap | 1u;
+    g.levels = 3;
+    auto front_for = [&](uint32_t rows) {
+      const uint64_t meta_cap = std::max<uint64_t>(static_cast<uint64_t>(tree_depth(rows)) * rows,
+                                                   static_cast<uint64_t>(g.levels) * rows + 2);
+      return static_cast<uint32_t>(round_up(std::max<uint64_t>(32 + 2 * meta_cap, cap), 4));
+    };
+    auto smem_for = [&](uint32_t rows) { return (front_for(rows) + 2ull * rows * g.pitch) * 4; };
+    uint32_t rows = 8;
+    while (rows < 65535 && smem_for(rows + 1) <= budget) ++rows;
+    g.max_rows = rows;
+    g.front = front_for(rows);
+    // R + 3 (2^K - 1) rows at the bottom of a column
+    while (g.levels > 1 && static_cast<int>(rows) - 3 * ((1 << g.levels) - 1) < 8) --g.levels;
+    g.block_rows = rows - 3 * ((1u << g.levels) - 1);
+    const uint32_t cp_pitch = (cap + P->max_width + 2) | 1u;
+    g.final_rows = std::min<uint32_t>(g.block_rows, (rows * g.pitch) / cp_pitch);
+    check_arg(g.final_rows >= 1 && g.block_rows >= 1, "FFA bins too large for the shared-memory tiles");
+    g.smem_bytes = smem_for(rows);
+    max_rows_all = std::max(max_rows_all, rows);
+  }
+  const uint32_t rows = max_rows_all;
+  // subtree schedules for every size up to max_rows
+  P->sub_offset.assign(rows + 1, 0u);
+  for (uint32_t n = 1; n <= rows; ++n) {
+    P->sub_offset[n] = static_cast<uint32_t>(P->sub_meta.size());
+    build_subtree_schedule(n, P->sub_meta);
+  }
+  if (P->sub_meta.empty()) P->sub_meta.push_back(MetaEntry{});
+  // tasks, trials, column schedules and classes
+  std::map<std::pair<int, uint32_t>, size_t> class_of;
+  for (uint64_t i = 0; i < P->tasks.size(); ++i) {
+    const auto& t = P->tasks[i];
+    const uint32_t m = P->task_member[i];
+    const FfaMember& M = P->members[m];
+    for (uint64_t w : M.widths)
+      check_arg(w > 0 && w < t.bins, "FFA detection width trials must satisfy 0 < width < bins");
+    TaskDev d{};
+    d.bins = static_cast<uint32_t>(t.bins);
+    d.rows = static_cast<uint32_t>(t.rows);
+    d.rows_eval = static_cast<uint32_t>(t.rows_eval);
+    d.octave = octave_of[m][t.downsample_factor];
+    d.prep_offset = M.octaves[d.octave].offset;
+    d.inv_stdnoise = 1.0f / task_stdnoise(t);
+    d.ntrials = static_cast<uint32_t>(M.widths.size());
+    d.trial_offset = static_cast<uint32_t>(P->trial_dev.size());
+    d.max_width = M.max_width;
+    d.member = m;
+    // ffa_detection.cpp:60-80 make_boxcar_trials (float arithmetic)
+    const float bf = static_cast<float>(t.bins);
+    for (uint64_t w : M.widths) {
+      const float wf = static_cast<float>(w);
+      const float h = std::sqrt((bf - wf) / (bf * wf));
+      P->trial_dev.push_back(TrialDev{h, wf / (bf - wf) * h, static_cast<uint32_t>(w), 0u});
     }
-    const uint32_t rows = max_rows_all;
-    // subtree schedules for every size up to max_rows
-    P->sub_offset.assign(rows + 1, 0u);
-    for (uint32_t n = 1; n <= rows; ++n) {
-      P->sub_offset[n] = static_cast<uint32_t>(P->sub_meta.size());
-      build_subtree_schedule(n, P->sub_meta);
+    const uint32_t nbt = static_cast<uint32_t>(ceil_div(t.bins, 32));
+    const FfaGeometry& g = P->geo[nbt];
+    uint32_t ds = 0;
+    while (ceil_div(t.rows, 1ull << ds) > g.max_rows) ++ds;
+    check_arg(ds <= 15, "FFA task too deep");
+    d.split_depth = ds;
+    if (ds > 0) build_task_passes(*P, g, d);
+    P->task_dev.push_back(d);
+    // cluster sized by rows for split tasks; on-chip tasks use key 0
+    int cluster = 1;
+    if (ds > 0) {
+      while (cluster < kClusterSize && static_cast<uint64_t>(cluster) * 512 < t.rows) cluster *= 2;
     }
-    if (P->sub_meta.empty()) P->sub_meta.push_back(MetaEntry{});
-    // tasks, trials, column schedules and classes
-    std::map<std::pair<int, uint32_t>, size_t> class_of;
-    for (uint64_t i = 0; i < ntasks; ++i) {
-      const auto& t = P->tasks[i];
-      for (uint64_t w : P->widths)
-        check_arg(w > 0 && w < t.bins, "FFA detection width trials must satisfy 0 < width < bins");
-      TaskDev d{};
-      d.bins = static_cast<uint32_t>(t.bins);
-      d.rows = static_cast<uint32_t>(t.rows);
-      d.rows_eval = static_cast<uint32_t>(t.rows_eval);
-      d.octave = octave_of[t.downsample_factor];
-      d.prep_offset = P->octaves[d.octave].offset;
-      d.inv_stdnoise = 1.0f / task_stdnoise(t);
-      d.ntrials = static_cast<uint32_t>(nwidths);
-      d.trial_offset = static_cast<uint32_t>(P->trial_dev.size());
-      d.max_width = P->max_width;
-      // ffa_detection.cpp:60-80 make_boxcar_trials (float arithmetic)
-      const float bf = static_cast<float>(t.bins);
-      for (uint64_t w : P->widths) {
-        const float wf = static_cast<float>(w);
-        const float h = std::sqrt((bf - wf) / (bf * wf));
-        P->trial_dev.push_back(TrialDev{h, wf / (bf - wf) * h, static_cast<uint32_t>(w), 0u});
-      }
-      const uint32_t nbt = static_cast<uint32_t>(ceil_div(t.bins, 32));
-      const FfaGeometry& g = P->geo[nbt];
-      uint32_t ds = 0;
-      while (ceil_div(t.rows, 1ull << ds) > g.max_rows) ++ds;
-      check_arg(ds <= 15, "FFA task too deep");
-      d.split_depth = ds;
-      if (ds > 0) build_task_passes(*P, g, d);
-      P->task_dev.push_back(d);
-      // cluster sized by rows for split tasks; on-chip tasks use key 0
-      int cluster = 1;
-      if (ds > 0) {
-        while (cluster < kClusterSize && static_cast<uint64_t>(cluster) * 512 < t.rows) cluster *= 2;
-      }
-      const uint32_t nb = static_cast<uint32_t>(ceil_div(t.bins, 32));
-      const std::pair<int, uint32_t> key{ds == 0 ? 0 : cluster, nb};
-      if (!class_of.count(key)) {
-        class_of[key] = P->classes.size();
-        P->classes.emplace_back();
-        P->classes.back().cluster = cluster;
-        P->classes.back().nb = nb;
-        P->classes.back().kernel = search_kernel_for(nb);
-      }
-      FfaClass& c = P->classes[class_of[key]];
-      c.tasks.push_back(static_cast<uint32_t>(i));
-      if (ds > 0) c.max_elems = std::max<uint64_t>(c.max_elems, t.rows * t.bins);
+    const uint32_t nb = static_cast<uint32_t>(ceil_div(t.bins, 32));
+    const std::pair<int, uint32_t> key{ds == 0 ? 0 : cluster, nb};
+    if (!class_of.count(key)) {
+      class_of[key] = P->classes.size();
+      P->classes.emplace_back();
+      P->classes.back().cluster = cluster;
+      P->classes.back().nb = nb;
+      P->classes.back().kernel = search_kernel_for(nb);
     }
-    // launch order: widest clusters (longest items) first
-    std::stable_sort(P->classes.begin(), P->classes.end(), [](const FfaClass& x, const FfaClass& y) {
-      return x.cluster != y.cluster ? x.cluster > y.cluster : x.nb > y.nb;
+    FfaClass& c = P->classes[class_of[key]];
+    c.tasks.push_back(static_cast<uint32_t>(i));
+    if (ds > 0) c.max_elems = std::max<uint64_t>(c.max_elems, t.rows * t.bins);
+  }
+  // launch order: widest clusters (longest items) first
+  std::stable_sort(P->classes.begin(), P->classes.end(), [](const FfaClass& x, const FfaClass& y) {
+    return x.cluster != y.cluster ? x.cluster > y.cluster : x.nb > y.nb;
+  });
+  if (P->col_meta.empty()) P->col_meta.resize(2);
+  if (P->blocks.empty()) P->blocks.resize(1);
+  if (P->passes.empty()) P->passes.resize(1);
+  for (auto& c : P->classes) {
+    // largest tasks first so long items start early
+    std::stable_sort(c.tasks.begin(), c.tasks.end(), [&](uint32_t x, uint32_t y) {
+      return P->tasks[x].rows * P->tasks[x].bins > P->tasks[y].rows * P->tasks[y].bins;
     });
-    if (P->col_meta.empty()) P->col_meta.resize(2);
-    if (P->blocks.empty()) P->blocks.resize(1);
-    if (P->passes.empty()) P->passes.resize(1);
-    int sms = 0;
-    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_id), "device attribute");
-    for (auto& c : P->classes) {
-      // largest tasks first so long items start early
-      std::stable_sort(c.tasks.begin(), c.tasks.end(), [&](uint32_t x, uint32_t y) {
-        return P->tasks[x].rows * P->tasks[x].bins > P->tasks[y].rows * P->tasks[y].bins;
-      });
-      const FfaGeometry& g = P->geo[c.nb];
-      cuda_check(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(g.smem_bytes)),
-                 "cudaFuncSetAttribute(ffa_search_kernel)");
-      cuda_check(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
-                 "cudaFuncSetAttribute(cluster size)");
-      cudaLaunchConfig_t cfg{};
-      cfg.gridDim = dim3(c.cluster, 1, 1);
-      cfg.blockDim = dim3(kThreads, 1, 1);
-      cfg.dynamicSmemBytes = g.smem_bytes;
-      cudaLaunchAttribute attr{};
-      attr.id = cudaLaunchAttributeClusterDimension;
-      attr.val.clusterDim.x = c.cluster;
-      attr.val.clusterDim.y = 1;
-      attr.val.clusterDim.z = 1;
-      cfg.attrs = &attr;
-      cfg.numAttrs = 1;
-      int n = 0;
-      cuda_check(cudaOccupancyMaxActiveClusters(&n, c.kernel, &cfg), "cudaOccupancyMaxActiveClusters");
-      check_arg(n > 0, "FFA kernel cannot be resident on this device");
-      c.nclusters = n;
-      // classes run one after another on the stream: they share the scratch
-      P->scratch_floats = std::max<uint64_t>(P->scratch_floats, static_cast<uint64_t>(n) * 2 * c.max_elems);
-      c.tasks_d.upload(c.tasks.data(), c.tasks.size() * sizeof(uint32_t), device_id);
+    if (batched) {
+      for (uint32_t task : c.tasks) {
+        const uint32_t m = P->task_member[task];
+        c.units.push_back(UnitDev{c.nitems, task, m});
+        c.nitems += P->members[m].nseries;
+      }
+      c.units_d.upload(c.units.data(), c.units.size() * sizeof(UnitDev), device_id);
     }
-    P->tasks_d.upload(P->task_dev.data(), P->task_dev.size() * sizeof(TaskDev), device_id);
-    P->trials_d.upload(P->trial_dev.data(), P->trial_dev.size() * sizeof(TrialDev), device_id);
-    P->octaves_d.upload(P->octaves.data(), P->octaves.size() * sizeof(OctaveDev), device_id);
-    P->sub_meta_d.upload(P->sub_meta.data(), P->sub_meta.size() * sizeof(MetaEntry), device_id);
-    P->sub_offset_d.upload(P->sub_offset.data(), P->sub_offset.size() * sizeof(uint32_t), device_id);
-    P->col_meta_d.upload(P->col_meta.data(), P->col_meta.size() * sizeof(MetaEntry), device_id);
-    P->blocks_d.upload(P->blocks.data(), P->blocks.size() * sizeof(ColBlock), device_id);
-    P->passes_d.upload(P->passes.data(), P->passes.size() * sizeof(PassDev), device_id);
-    *out = P.release();
+    const FfaGeometry& g = P->geo[c.nb];
+    cuda_check(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(g.smem_bytes)),
+               "cudaFuncSetAttribute(ffa_search_kernel)");
+    cuda_check(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+               "cudaFuncSetAttribute(cluster size)");
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(c.cluster, 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = g.smem_bytes;
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = c.cluster;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    cuda_check(cudaOccupancyMaxActiveClusters(&n, c.kernel, &cfg), "cudaOccupancyMaxActiveClusters");
+    check_arg(n > 0, "FFA kernel cannot be resident on this device");
+    c.nclusters = n;
+    // classes run one after another on the stream: they share the scratch
+    P->scratch_floats = std::max<uint64_t>(P->scratch_floats, static_cast<uint64_t>(n) * 2 * c.max_elems);
+    c.tasks_d.upload(c.tasks.data(), c.tasks.size() * sizeof(uint32_t), device_id);
+  }
+  P->tasks_d.upload(P->task_dev.data(), P->task_dev.size() * sizeof(TaskDev), device_id);
+  P->trials_d.upload(P->trial_dev.data(), P->trial_dev.size() * sizeof(TrialDev), device_id);
+  for (auto& M : P->members) M.octaves_d.upload(M.octaves.data(), M.octaves.size() * sizeof(OctaveDev), device_id);
+  P->sub_meta_d.upload(P->sub_meta.data(), P->sub_meta.size() * sizeof(MetaEntry), device_id);
+  P->sub_offset_d.upload(P->sub_offset.data(), P->sub_offset.size() * sizeof(uint32_t), device_id);
+  P->col_meta_d.upload(P->col_meta.data(), P->col_meta.size() * sizeof(MetaEntry), device_id);
+  P->blocks_d.upload(P->blocks.data(), P->blocks.size() * sizeof(ColBlock), device_id);
+  P->passes_d.upload(P->passes.data(), P->passes.size() * sizeof(PassDev), device_id);
+  return P;
+}
+
+void launch_prepare(const gf_ffa_program* P, const FfaMember& M, const float* dev_series, uint64_t nseries,
+                    uint64_t stride, const double* dev_stats, float* dev_prepared, cudaStream_t s) {
+  check_arg(dev_series && dev_prepared, "null argument");
+  check_arg(nseries > 0 && nseries < 65536, "nseries out of range");
+  check_arg(stride >= M.nsamples, "stride must be >= nsamples");
+  DeviceGuard dg(P->device);
+  const size_t smem = (kPrepareChunk + M.halo) * sizeof(float);
+  check_arg(smem <= 200 * 1024, "downsample factor too large for the prepare kernel");
+  cuda_check(cudaFuncSetAttribute(prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)),
+             "cudaFuncSetAttribute(prepare_kernel)");
+  dim3 grid(static_cast<unsigned>(ceil_div(M.nsamples, kPrepareChunk)), static_cast<unsigned>(nseries));
+  prepare_kernel<<<grid, kThreads, smem, s>>>(dev_series, stride, M.nsamples, dev_stats,
+                                              M.octaves_d.as<OctaveDev>(), static_cast<int>(M.octaves.size()),
+                                              M.halo, dev_prepared, M.prep_stride);
+  cuda_check(cudaGetLastError(), "prepare_kernel launch");
+}
+
+// One launch per class; batched programs walk their item runs.
+void launch_search(gf_ffa_program* P, const float* dev_prepared, uint64_t nseries, float snr_threshold,
+                   void* dev_scratch, gf_peak_record* dev_peaks, uint64_t capacity, uint64_t* dev_counters,
+                   cudaStream_t s) {
+  check_arg(dev_counters, "null argument");
+  check_arg(std::isfinite(snr_threshold), "FFA search S/N threshold must be finite");
+  check_arg(capacity == 0 || dev_peaks != nullptr, "peak buffer must not be null");
+  check_arg(P->scratch_floats == 0 || dev_scratch != nullptr, "FFA search needs scratch");
+  DeviceGuard dg(P->device);
+  cuda_check(cudaMemsetAsync(dev_counters, 0, 2 * sizeof(uint64_t), s), "cudaMemsetAsync(counters)");
+  SearchParams sp{};
+  sp.prepared = dev_prepared;
+  sp.prep_stride = P->members[0].prep_stride;
+  sp.tasks = P->tasks_d.as<TaskDev>();
+  sp.trials = P->trials_d.as<TrialDev>();
+  sp.sub_meta = P->sub_meta_d.as<MetaEntry>();
+  sp.sub_offset = P->sub_offset_d.as<uint32_t>();
+  sp.nseries = static_cast<uint32_t>(nseries);
+  sp.members = P->batched ? P->members_d.as<MemberDev>() : nullptr;
+  sp.threshold = snr_threshold;
+  sp.peaks = dev_peaks;
+  sp.capacity = capacity;
+  sp.counters = reinterpret_cast<unsigned long long*>(dev_counters);
+  sp.col_meta = P->col_meta_d.as<MetaEntry>();
+  sp.blocks = P->blocks_d.as<ColBlock>();
+  sp.passes = P->passes_d.as<PassDev>();
+  sp.scratch = static_cast<float*>(dev_scratch);
+  for (const FfaClass& c : P->classes) {
+    sp.item_tasks = c.tasks_d.as<uint32_t>();
+    sp.nitem_tasks = static_cast<uint32_t>(c.tasks.size());
+    sp.units = P->batched ? c.units_d.as<UnitDev>() : nullptr;
+    sp.nunits = static_cast<uint32_t>(c.units.size());
+    sp.nitems = c.nitems;
+    sp.scratch_elems = c.max_elems;
+    const FfaGeometry& g = P->geo[c.nb];
+    sp.pitch = g.pitch;
+    sp.max_rows = g.max_rows;
+    sp.front = g.front;
+    const uint64_t items = P->batched ? c.nitems : nseries * c.tasks.size();
+    if (items == 0) continue;
+    const unsigned nclusters = static_cast<unsigned>(std::min<uint64_t>(items, static_cast<uint64_t>(c.nclusters)));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(nclusters * c.cluster, 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = g.smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = c.cluster;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    cuda_check(cudaLaunchKernelEx(&cfg, c.kernel, sp), "ffa_search_kernel launch");
+  }
+}
+
+// make_ffa_peak (ffa_detection.cpp:266-284) with trial_period
+// (ffa_detection.cpp:115-124); dm = dm_low + (series_offset + series) * dm_step
+void expand_record(const gf_ffa_program* P, const gf_peak_record& r, uint64_t series_offset, double dm_low,
+                   double dm_step, gf_peak& p) {
+  check_arg(r.task < P->tasks.size(), "corrupt peak record");
+  const FfaMember& M = P->members[P->task_member[r.task]];
+  check_arg(r.width_index < M.widths.size(), "corrupt peak record");
+  const gf_ffa_task& t = P->tasks[r.task];
+  double period;
+  if (t.rows <= 1) {
+    period = t.effective_tsamp * static_cast<double>(t.bins);
+  } else {
+    const double b = static_cast<double>(t.bins);
+    period = t.effective_tsamp * b * b / (b - static_cast<double>(r.shift) / static_cast<double>(t.rows - 1));
+  }
+  const uint64_t series = series_offset + r.series;
+  p.dm = dm_low + static_cast<double>(series) * dm_step;
+  p.dm_index = series;
+  p.period = period;
+  p.frequency = 1.0 / period;
+  p.width = M.widths[r.width_index];
+  p.duty_cycle = static_cast<double>(p.width) / static_cast<double>(t.bins);
+  p.width_index = r.width_index;
+  p.period_index = r.shift;
+  p.phase = r.phase;
+  p.shift = r.shift;
+  p.bins = t.bins;
+  p.snr = r.snr;
+  p.reserved = 0;
+}
+
+}  // namespace
+
+extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, const uint64_t* widths,
+                                     uint64_t nwidths, uint64_t max_series, int32_t device_id,
+                                     gf_ffa_program** out) {
+  return guarded([&] {
+    check_arg(out != nullptr, "null argument");
+    *out = nullptr;
+    check_arg(max_series > 0 && max_series < (1ull << 31), "max_series out of range");
+    DeviceGuard dg(device_id);
+    *out = build_program({MemberSpec{tasks, ntasks, widths, nwidths, max_series}}, false, max_series, device_id)
+               .release();
+  });
+}
+
+extern "C" int gf_ffa_batch_create(const gf_ffa_batch_member* members, uint64_t nmembers, int32_t device_id,
+                                   gf_ffa_program** out) {
+  return guarded([&] {
+    check_arg(members && out, "null argument");
+    *out = nullptr;
+    check_arg(nmembers > 0 && nmembers < 65536, "batched FFA programs hold 1 to 65535 members");
+    std::vector<MemberSpec> specs;
+    uint64_t mx = 0;
+    for (uint64_t m = 0; m < nmembers; ++m) {
+      const gf_ffa_batch_member& b = members[m];
+      check_arg(b.nseries > 0 && b.nseries < 65536, "member nseries out of range");
+      specs.push_back(MemberSpec{b.tasks, b.ntasks, b.widths, b.nwidths, b.nseries});
+      mx = std::max(mx, b.nseries);
+    }
+    DeviceGuard dg(device_id);
+    *out = build_program(specs, true, mx, device_id).release();
   });
 }
 
@@ -1121,36 +1341,44 @@ extern "C" int gf_ffa_program_info(const gf_ffa_program* P, gf_ffa_info* info) {
     check_arg(P && info, "null argument");
     std::memset(info, 0, sizeof *info);
     info->ntasks = P->tasks.size();
-    info->noctaves = P->octaves.size();
-    info->prepared_floats = P->prep_stride;
+    for (const auto& M : P->members) {
+      info->noctaves = std::max<uint64_t>(info->noctaves, M.octaves.size());
+      info->prepared_floats = std::max<uint64_t>(info->prepared_floats, M.prep_stride);
+    }
     info->scratch_bytes = std::max<uint64_t>(16, P->scratch_floats * 4);
     uint64_t mx = 0;
     for (const auto& t : P->tasks) mx = std::max<uint64_t>(mx, t.rows * t.bins);
     info->max_task_elements = mx;
-    info->metadata_bytes = P->tasks_d.bytes + P->trials_d.bytes + P->octaves_d.bytes + P->sub_meta_d.bytes +
-                           P->sub_offset_d.bytes + P->col_meta_d.bytes + P->blocks_d.bytes + P->passes_d.bytes;
-    for (const auto& c : P->classes) info->metadata_bytes += c.tasks_d.bytes;
+    info->metadata_bytes = P->tasks_d.bytes + P->trials_d.bytes + P->sub_meta_d.bytes + P->sub_offset_d.bytes +
+                           P->col_meta_d.bytes + P->blocks_d.bytes + P->passes_d.bytes + P->members_d.bytes;
+    for (const auto& M : P->members) info->metadata_bytes += M.octaves_d.bytes;
+    for (const auto& c : P->classes) info->metadata_bytes += c.tasks_d.bytes + c.units_d.bytes;
     info->nclasses = P->classes.size();
+  });
+}
+
+extern "C" int gf_ffa_batch_member_info(const gf_ffa_program* P, uint64_t member,
+                                        gf_ffa_member_info* info) {
+  return guarded([&] {
+    check_arg(P && info, "null argument");
+    check_arg(member < P->members.size(), "member out of range");
+    const FfaMember& M = P->members[member];
+    std::memset(info, 0, sizeof *info);
+    info->nsamples = M.nsamples;
+    info->nseries = M.nseries;
+    info->prepared_floats = M.prep_stride;
+    info->task_begin = M.task_begin;
+    info->ntasks = M.ntasks;
+    info->noctaves = M.octaves.size();
   });
 }
 
 extern "C" int gf_ffa_prepare(gf_ffa_program* P, const float* dev_series, uint64_t nseries, uint64_t stride,
                               const double* dev_stats, float* dev_prepared, void* stream) {
   return guarded([&] {
-    check_arg(P && dev_series && dev_prepared, "null argument");
-    check_arg(nseries > 0 && nseries < 65536, "nseries out of range");
-    check_arg(stride >= P->nsamples, "stride must be >= nsamples");
-    DeviceGuard dg(P->device);
-    const size_t smem = (kPrepareChunk + P->halo) * sizeof(float);
-    check_arg(smem <= 200 * 1024, "downsample factor too large for the prepare kernel");
-    cuda_check(cudaFuncSetAttribute(prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)),
-               "cudaFuncSetAttribute(prepare_kernel)");
-    dim3 grid(static_cast<unsigned>(ceil_div(P->nsamples, kPrepareChunk)), static_cast<unsigned>(nseries));
-    prepare_kernel<<<grid, kThreads, smem, as_stream(stream)>>>(
-        dev_series, stride, P->nsamples, dev_stats, P->octaves_d.as<OctaveDev>(),
-        static_cast<int>(P->octaves.size()), P->halo, dev_prepared, P->prep_stride);
-    cuda_check(cudaGetLastError(), "prepare_kernel launch");
+    check_arg(P != nullptr, "null argument");
+    check_arg(!P->batched, "batched FFA programs prepare through gf_ffa_batch_prepare");
+    launch_prepare(P, P->members[0], dev_series, nseries, stride, dev_stats, dev_prepared, as_stream(stream));
   });
 }
 
@@ -1158,54 +1386,52 @@ extern "C" int gf_ffa_search(gf_ffa_program* P, const float* dev_prepared, uint6
                              void* dev_scratch, gf_peak_record* dev_peaks, uint64_t capacity,
                              uint64_t* dev_counters, void* stream) {
   return guarded([&] {
-    check_arg(P && dev_prepared && dev_counters, "null argument");
-    check_arg(std::isfinite(snr_threshold), "FFA search S/N threshold must be finite");
+    check_arg(P && dev_prepared, "null argument");
+    check_arg(!P->batched, "batched FFA programs search through gf_ffa_batch_search");
     check_arg(nseries > 0 && nseries <= P->max_series, "nseries must be in (0, max_series]");
-    check_arg(capacity == 0 || dev_peaks != nullptr, "peak buffer must not be null");
-    check_arg(P->scratch_floats == 0 || dev_scratch != nullptr, "FFA search needs scratch");
+    launch_search(P, dev_prepared, nseries, snr_threshold, dev_scratch, dev_peaks, capacity, dev_counters,
+                  as_stream(stream));
+  });
+}
+
+extern "C" int gf_ffa_batch_bind(gf_ffa_program* P, const float* const* dev_prepared) {
+  return guarded([&] {
+    check_arg(P && dev_prepared, "null argument");
+    check_arg(P->batched, "gf_ffa_batch_bind needs a batched FFA program");
     DeviceGuard dg(P->device);
-    auto s = as_stream(stream);
-    cuda_check(cudaMemsetAsync(dev_counters, 0, 2 * sizeof(uint64_t), s), "cudaMemsetAsync(counters)");
-    SearchParams sp{};
-    sp.prepared = dev_prepared;
-    sp.prep_stride = P->prep_stride;
-    sp.tasks = P->tasks_d.as<TaskDev>();
-    sp.trials = P->trials_d.as<TrialDev>();
-    sp.sub_meta = P->sub_meta_d.as<MetaEntry>();
-    sp.sub_offset = P->sub_offset_d.as<uint32_t>();
-    sp.nseries = static_cast<uint32_t>(nseries);
-    sp.threshold = snr_threshold;
-    sp.peaks = dev_peaks;
-    sp.capacity = capacity;
-    sp.counters = reinterpret_cast<unsigned long long*>(dev_counters);
-    sp.col_meta = P->col_meta_d.as<MetaEntry>();
-    sp.blocks = P->blocks_d.as<ColBlock>();
-    sp.passes = P->passes_d.as<PassDev>();
-    sp.scratch = static_cast<float*>(dev_scratch);
-    for (const FfaClass& c : P->classes) {
-      sp.item_tasks = c.tasks_d.as<uint32_t>();
-      sp.nitem_tasks = static_cast<uint32_t>(c.tasks.size());
-      sp.scratch_elems = c.max_elems;
-      const FfaGeometry& g = P->geo[c.nb];
-      sp.pitch = g.pitch;
-      sp.max_rows = g.max_rows;
-      sp.front = g.front;
-      const uint64_t items = nseries * c.tasks.size();
-      const unsigned nclusters = static_cast<unsigned>(std::min<uint64_t>(items, static_cast<uint64_t>(c.nclusters)));
-      cudaLaunchConfig_t cfg{};
-      cfg.gridDim = dim3(nclusters * c.cluster, 1, 1);
-      cfg.blockDim = dim3(kThreads, 1, 1);
-      cfg.dynamicSmemBytes = g.smem_bytes;
-      cfg.stream = s;
-      cudaLaunchAttribute attr{};
-      attr.id = cudaLaunchAttributeClusterDimension;
-      attr.val.clusterDim.x = c.cluster;
-      attr.val.clusterDim.y = 1;
-      attr.val.clusterDim.z = 1;
-      cfg.attrs = &attr;
-      cfg.numAttrs = 1;
-      cuda_check(cudaLaunchKernelEx(&cfg, c.kernel, sp), "ffa_search_kernel launch");
+    std::vector<MemberDev> md(P->members.size());
+    for (size_t m = 0; m < P->members.size(); ++m) {
+      check_arg(dev_prepared[m] != nullptr, "null prepared buffer");
+      check_arg((reinterpret_cast<uintptr_t>(dev_prepared[m]) & 15u) == 0,
+                "prepared buffers must be 16-byte aligned");
+      P->members[m].prepared = dev_prepared[m];
+      md[m] = MemberDev{dev_prepared[m], P->members[m].prep_stride};
     }
+    P->members_d.upload(md.data(), md.size() * sizeof(MemberDev), P->device);
+    P->bound = true;
+  });
+}
+
+extern "C" int gf_ffa_batch_prepare(gf_ffa_program* P, uint64_t member, const float* dev_series, uint64_t stride,
+                                    const double* dev_stats, void* stream) {
+  return guarded([&] {
+    check_arg(P != nullptr, "null argument");
+    check_arg(P->batched && P->bound, "gf_ffa_batch_prepare needs a bound batched FFA program");
+    check_arg(member < P->members.size(), "member out of range");
+    const FfaMember& M = P->members[member];
+    launch_prepare(P, M, dev_series, M.nseries, stride, dev_stats, const_cast<float*>(M.prepared),
+                   as_stream(stream));
+  });
+}
+
+extern "C" int gf_ffa_batch_search(gf_ffa_program* P, float snr_threshold, void* dev_scratch,
+                                   gf_peak_record* dev_peaks, uint64_t capacity, uint64_t* dev_counters,
+                                   void* stream) {
+  return guarded([&] {
+    check_arg(P != nullptr, "null argument");
+    check_arg(P->batched && P->bound, "gf_ffa_batch_search needs a bound batched FFA program");
+    launch_search(P, nullptr, 0, snr_threshold, dev_scratch, dev_peaks, capacity, dev_counters,
+                  as_stream(stream));
   });
 }
 
@@ -1213,33 +1439,22 @@ extern "C" int gf_ffa_expand_peaks(const gf_ffa_program* P, const gf_peak_record
                                    uint64_t series_offset, double dm_low, double dm_step, gf_peak* out) {
   return guarded([&] {
     check_arg(P && (n == 0 || (records && out)), "null argument");
+    for (uint64_t i = 0; i < n; ++i) expand_record(P, records[i], series_offset, dm_low, dm_step, out[i]);
+  });
+}
+
+extern "C" int gf_ffa_batch_expand_peaks(const gf_ffa_program* P, const gf_peak_record* records, uint64_t n,
+                                         const uint64_t* series_offset, const double* dm_low,
+                                         const double* dm_step, gf_peak* out, uint32_t* member) {
+  return guarded([&] {
+    check_arg(P && (n == 0 || (records && out && member && series_offset && dm_low && dm_step)),
+              "null argument");
     for (uint64_t i = 0; i < n; ++i) {
-      const gf_peak_record& r = records[i];
-      check_arg(r.task < P->tasks.size() && r.width_index < P->widths.size(), "corrupt peak record");
-      const gf_ffa_task& t = P->tasks[r.task];
-      // ffa_detection.cpp:115-124 trial_period, :266-284 make_ffa_peak
-      double period;
-      if (t.rows <= 1) {
-        period = t.effective_tsamp * static_cast<double>(t.bins);
-      } else {
-        const double b = static_cast<double>(t.bins);
-        period = t.effective_tsamp * b * b / (b - static_cast<double>(r.shift) / static_cast<double>(t.rows - 1));
-      }
-      gf_peak& p = out[i];
-      const uint64_t series = series_offset + r.series;
-      p.dm = dm_low + static_cast<double>(series) * dm_step;
-      p.dm_index = series;
-      p.period = period;
-      p.frequency = 1.0 / period;
-      p.width = P->widths[r.width_index];
-      p.duty_cycle = static_cast<double>(p.width) / static_cast<double>(t.bins);
-      p.width_index = r.width_index;
-      p.period_index = r.shift;
-      p.phase = r.phase;
-      p.shift = r.shift;
-      p.bins = t.bins;
-      p.snr = r.snr;
-      p.reserved = 0;
+      check_arg(records[i].task < P->tasks.size(), "corrupt peak record");
+      const uint32_t m = P->task_member[records[i].task];
+      check_arg(records[i].series < P->members[m].nseries, "corrupt peak record");
+      expand_record(P, records[i], series_offset[m], dm_low[m], dm_step[m], out[i]);
+      member[i] = m;
     }
   });
 }

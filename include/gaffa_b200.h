@@ -115,6 +115,8 @@ typedef struct {
   uint64_t subband_channels; /* subband only */
   uint64_t ndm_per_nominal;  /* subband only */
   int32_t device_id;
+  int32_t launch_dms_per_cta; /* brute force launch shape, 0 = automatic: DMs per CTA (1, 2, 4, 8) */
+  int32_t launch_chunk_rows;  /* 0 = automatic: channel rows staged per step (8, 16, 32, 64) */
   int32_t reserved;
 } gf_dedisp_desc;
 
@@ -159,6 +161,26 @@ int gf_dedisp_stage_from_host(gf_dedisp_program* program, const void* host_input
 int gf_dedisp_run(gf_dedisp_program* program, const void* dev_staged,
                   uint64_t dm_begin, uint64_t dm_count, uint32_t* dev_out,
                   uint64_t out_stride, void* dev_workspace, void* stream);
+/* Batched brute-force dedispersion: many (program, DM range) items, of
+ * different observations, channel counts and lengths, in one launch.  The
+ * reference launches multi_dm_kernel once per plan (dedispersion_cuda.cu:
+ * 536-585); each item's output is identical to gf_dedisp_run of the same
+ * range.  Pointers are fixed at creation, so gf_dedisp_batch_run can be
+ * captured in a CUDA graph. */
+typedef struct gf_dedisp_batch gf_dedisp_batch;
+typedef struct {
+  const gf_dedisp_program* program;   /* brute force */
+  const void* dev_staged;             /* the program's staged filterbank */
+  uint64_t dm_begin;                  /* multiple of 8 */
+  uint64_t dm_count;
+  uint32_t* dev_out;                  /* [dm_count][out_stride] */
+  uint64_t out_stride;
+} gf_dedisp_batch_item;
+int gf_dedisp_batch_create(const gf_dedisp_batch_item* items, uint64_t nitems,
+                           gf_dedisp_batch** out);
+int gf_dedisp_batch_run(gf_dedisp_batch* batch, void* stream);
+int gf_dedisp_batch_destroy(gf_dedisp_batch* batch);
+
 /* Workspace bytes gf_dedisp_run needs for a batch of dm_count DMs (0 for
  * brute force; the subband intermediate otherwise).  Brute-force batches start
  * at multiples of 8 DMs, subband batches at multiples of ndm_per_nominal. */
@@ -350,6 +372,53 @@ int gf_ffa_expand_peaks(const gf_ffa_program* program,
                         const gf_peak_record* records, uint64_t n,
                         uint64_t series_offset, double dm_low, double dm_step,
                         gf_peak* out);
+
+/* Batched FFA search: the plans of many observations (members) in one
+ * program, so each launch class covers every member's (series, task) items
+ * in one persistent launch.  The reference runs one CudaFfaProgram per
+ * observation (ffa_cuda_executor.cuh:44-80, run_ffa_batch_cuda :672-678);
+ * results are identical to searching each member with its own program.
+ * Records name the global task (task_begin of its member + local index) and
+ * the series within the member. */
+typedef struct {
+  const gf_ffa_task* tasks;
+  uint64_t ntasks;
+  const uint64_t* widths;
+  uint64_t nwidths;
+  uint64_t nseries;             /* series searched per gf_ffa_batch_search */
+} gf_ffa_batch_member;
+
+typedef struct {
+  uint64_t nsamples;
+  uint64_t nseries;
+  uint64_t prepared_floats;     /* per series, all octaves */
+  uint64_t task_begin;          /* first global task index of the member */
+  uint64_t ntasks;
+  uint64_t noctaves;
+} gf_ffa_member_info;
+
+int gf_ffa_batch_create(const gf_ffa_batch_member* members, uint64_t nmembers,
+                        int32_t device_id, gf_ffa_program** out);
+int gf_ffa_batch_member_info(const gf_ffa_program* program, uint64_t member,
+                             gf_ffa_member_info* info);
+/* dev_prepared: host array of nmembers device pointers, each
+ * [nseries][prepared_floats] floats, 16-byte aligned.  Synchronous upload;
+ * call before capturing launches into a CUDA graph. */
+int gf_ffa_batch_bind(gf_ffa_program* program, const float* const* dev_prepared);
+/* prepare_ffa_input_cuda of one member's nseries series into its bound buffer. */
+int gf_ffa_batch_prepare(gf_ffa_program* program, uint64_t member,
+                         const float* dev_series, uint64_t stride,
+                         const double* dev_stats, void* stream);
+/* One launch per class over every member; no host synchronisation. */
+int gf_ffa_batch_search(gf_ffa_program* program, float snr_threshold,
+                        void* dev_scratch, gf_peak_record* dev_peaks,
+                        uint64_t capacity, uint64_t* dev_counters, void* stream);
+/* gf_ffa_expand_peaks with per-member series offsets and DM grids; member[i]
+ * receives the record's member. */
+int gf_ffa_batch_expand_peaks(const gf_ffa_program* program,
+                              const gf_peak_record* records, uint64_t n,
+                              const uint64_t* series_offset, const double* dm_low,
+                              const double* dm_step, gf_peak* out, uint32_t* member);
 
 /* One materialised FFA transform of [rows][bins] floats (ffa_transform_cpu /
  * ffa_transform_block_cuda, ffa.cpp:342-417, ffa_cuda.h:254-264).
