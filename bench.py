@@ -54,6 +54,11 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU baseline sample time")
+    ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal measurement")
+    ap.add_argument("--proposal-fraction", type=float, default=None,
+                    help="fraction of DM windows searched (default: the shipped model's)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven-workload measurement")
+    ap.add_argument("--batched-observations", type=int, default=12)
     return ap.parse_args()
 
 
@@ -217,6 +222,95 @@ def run_reference(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def proposal_measurement(cfg, ds, raw, exhaustive, fraction):
+    """The learned-proposal path on the same observation: the coarse search,
+    the network's window scores, then the full-resolution search of the top
+    fraction of DM windows.  Throughput counts every DM trial of the
+    observation (the ones the proposal rules out included); recall is over
+    the injections the exhaustive search itself detected."""
+    import torch
+    from gaffa_b200 import proposal
+    obs = cfg.obs
+    dev = ds.device.index or 0
+    net = proposal.ProposalNet(device_id=dev)
+    meta = net.load_default()
+    frac = fraction if fraction is not None else meta["fraction"]
+    dm_max = cfg.dm_low + (cfg.ndm - 1) * cfg.dm_step
+    cf = proposal.CoarseFeatures(obs.frequencies, obs.nsamples, obs.tsamp, dm_max, device_id=dev)
+
+    def run_once():
+        feats = cf(raw)
+        scores = net.forward(feats)
+        windows = proposal.select_windows(scores, frac)
+        ranges = proposal.dm_ranges_for_windows(windows, cfg.ndm, cfg.dm_step, dm_max, ds.dedisp.batch_granularity)
+        return feats, windows, ranges, ds.run(raw, dm_ranges=ranges)
+
+    run_once()  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    feats, windows, ranges, _ = run_once()
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    det = proposal.detected_injections(exhaustive.candidates, obs.pulsars, obs.nsamples * obs.tsamp,
+                                       cfg.snr_threshold, proposal.band_delay_per_dm(obs.frequencies))
+    found, total = proposal.injection_recall(det, windows, dm_max)
+    hfound, _ = proposal.injection_recall(det, proposal.select_windows(proposal.baseline_scores(feats), frac),
+                                          dm_max)
+    return {"value": cfg.ndm * ds.nout / sec, "unit": UNIT, "ms_per_step": sec * 1e3, "window_fraction": frac,
+            "dm_trials_searched": int(sum(e - b for b, e in ranges)), "injections_detected_exhaustive": total,
+            "injections_recalled": found, "recall": (found / total) if total else None,
+            "heuristic_recalled_same_budget": hfound, "model": meta.get("trained_on", ""),
+            "model_val_recall_at_fraction": meta.get("val_recall_at_fraction")}
+
+
+def batched_measurement(nobs: int, device_id: int) -> dict:
+    """The batched uneven workload at reduced size: nobs observations with the
+    batched laws (channels from {1024, 2048, 4096}, lengths log-uniform over
+    2^18-2^20, 256-1024 DM trials over 0-1000, own FFA period ranges).  Times
+    one batched run (one dedispersion launch and one FFA launch per class per
+    wave, replayed from captured CUDA graphs, autotuned dedispersion shapes)
+    against the same observations searched one after another by DmSearch,
+    both from HBM-resident filterbanks, and checks that the peaks agree."""
+    import numpy as np
+    import torch
+    from gaffa_b200 import batch, configs, core, search
+    cs = configs.batched_uneven(seed=0, nobs=nobs, log2_nsamples=(18.0, 20.0), ndm_range=(256, 1024))
+    data = [core.synth_generate(c.obs, device_id=device_id) for c in cs]
+    tuner = batch.Autotuner()
+    t0 = time.perf_counter()
+    bs = batch.BatchSearch(cs, device_id=device_id, tuner=tuner)
+    first = bs.run(data)                       # tunes, builds the waves, captures the graphs
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    units = sum(c.ndm * dd.nout for c, dd in zip(cs, bs.dd))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - a, out
+
+    sec_replay, got = timed(lambda: bs.run())         # staged data resident: graph replays only
+    sec_b, _ = timed(lambda: bs.run(data))           # with the staging of every filterbank
+    searches = [search.from_config(c, device_id=device_id) for c in cs]
+    for s, x in zip(searches, data):
+        s.run(x)                                     # warm-up
+    sec_s, want = timed(lambda: [s.run(x) for s, x in zip(searches, data)])
+    same = all(np.array_equal(a.peaks, b.peaks) and np.array_equal(a.candidates, b.candidates)
+               for a, b in zip(got, want)) and all(np.array_equal(a.peaks, b.peaks) for a, b in zip(first, want))
+    waves = len(bs.waves)
+    launches = bs.kernel_launches_per_run
+    del bs, searches, data
+    torch.cuda.empty_cache()
+    return {"value": units / sec_b, "unit": UNIT, "observations": nobs, "dm_trial_samples": units, "waves": waves,
+            "kernel_launches_per_run": launches, "seconds": sec_b, "seconds_staged_data": sec_replay,
+            "sequential_value": units / sec_s, "sequential_seconds": sec_s, "speedup_vs_sequential": sec_s / sec_b,
+            "identical_to_sequential": bool(same), "setup_seconds": setup,
+            "tuned_dedispersion_shapes": tuner.cache,
+            "config": "batched uneven laws at 2^18-2^20 samples and 256-1024 DM trials"}
+
+
 def cpu_baseline(cfg, host_input, seconds: float) -> dict:
     from oracle.oracle import Oracle
     kind = "reference" if Oracle.available("reference") else "port"
@@ -269,6 +363,9 @@ def main():
     from gaffa_b200 import core, search
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = batched_measurement(args.batched_observations, local)
     cfg = workload(args, rank)
     obs = cfg.obs
     raw = core.synth_generate(obs, device_id=local)          # device-resident filterbank
@@ -348,6 +445,14 @@ def main():
         e2e = {"value": units * world / (ms_e2e / 1e3), "unit": UNIT, "ms_per_step": ms_e2e,
                "h2d_bytes_per_step": int(raw.numel()), "d2h_bytes_per_step": d2h}
 
+    prop = None
+    if rank == 0 and world == 1 and not args.no_proposal:
+        try:
+            prop = proposal_measurement(cfg, ds, raw, res, args.proposal_fraction)
+            prop["speedup_vs_plain"] = prop["value"] / value
+        except FileNotFoundError as exc:
+            prop = {"unavailable": f"no trained proposal model: {exc}"}
+
     baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         src = host.numpy() if host is not None else raw.cpu().numpy()
@@ -372,6 +477,8 @@ def main():
             "gpu_launches": res.gpu_launches * args.steps,
             "roofline": roofline,
             "cpu_baseline": baseline,
+            "proposal": prop,
+            "batched": batched,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

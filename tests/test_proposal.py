@@ -63,6 +63,30 @@ def test_labels_windows_and_octaves():
     assert proposal.recall(c, [0], 1000.0, 8.0) == (1, 2)
 
 
+def test_injection_matching_labels_and_recall():
+    from gaffa_b200 import _lib, proposal, synth
+    psr = [synth.Pulsar(period=0.5, dm=300.0, duty_cycle=0.02, amplitude=1.0),
+           synth.Pulsar(period=2.0, dm=900.0, duty_cycle=0.02, amplitude=1.0)]
+    c = np.zeros(5, _lib.CAND_DTYPE)
+    c["dm"] = [300.5, 301.0, 600.0, 299.0, 900.0]
+    c["period"] = [0.5, 0.25, 0.5, 1.5, 2.0]       # fundamental, 2nd harmonic, wrong DM, 1/3, S/N too low
+    c["frequency"] = 1.0 / c["period"]
+    c["snr"] = [12.0, 9.0, 15.0, 8.5, 7.0]
+    band = 4148.808 * (1 / 1100.0 ** 2 - 1 / 1700.0 ** 2)   # ~2 ms per unit DM
+    det = proposal.detected_injections(c, psr, 67.0, 8.0, band)
+    assert sorted(det[0]["dm"]) == [299.0, 300.5, 301.0] and len(det[1]) == 0
+    y = proposal.labels_from_detections(psr, det, 1000.0)
+    w = proposal.window_of_dm(300.0, 1000.0)
+    assert y[w, 4] == 1 and y[w, 5] == 1 and y[w, 3] == 1 and y.sum() == 3   # 0.5 s, 0.25 s, 1.5 s
+    assert proposal.injection_recall(det, [w], 1000.0) == (1, 1)
+    assert proposal.injection_recall(det, [w + 2], 1000.0) == (0, 1)
+    torch = pytest.importorskip("torch")
+    f = torch.zeros((proposal.NCOARSE, proposal.IN_CHANNELS, proposal.NBINS))
+    f[7, 0, 100] = 2.0
+    f[9, 0, 3] = 1.0
+    assert list(proposal.select_windows(proposal.baseline_scores(f), 2 / proposal.NCOARSE)) == [7, 9]
+
+
 @pytest.mark.gpu
 def test_cuda_forward_and_gradients_match_oracle():
     import torch
@@ -70,7 +94,8 @@ def test_cuda_forward_and_gradients_match_oracle():
     rng = np.random.default_rng(2)
     net = proposal.ProposalNet(seed=3)
     B, L = 3, proposal.NBINS
-    feat = torch.from_numpy(rng.normal(0, 1, (B, 32, L)).astype(np.float32)).cuda().to(torch.bfloat16)
+    feat = torch.from_numpy(rng.normal(0, 1, (B, proposal.IN_CHANNELS, L)).astype(np.float32)).cuda().to(
+        torch.bfloat16)
     labels = torch.from_numpy((rng.random((B, OCT)) < 0.3).astype(np.float32)).cuda()
     loss, grads, logits = net.loss_and_grads(feat, labels, 7.0)
     ws = [w.cpu().double().numpy() for w in net.w]
@@ -94,7 +119,7 @@ def test_training_reduces_loss_on_fixed_batch():
     rng = np.random.default_rng(4)
     net = proposal.ProposalNet(seed=5)
     B = 32
-    feat = torch.from_numpy(rng.normal(0, 1, (B, 32, proposal.NBINS)).astype(np.float32))
+    feat = torch.from_numpy(np.abs(rng.normal(0, 1, (B, proposal.IN_CHANNELS, proposal.NBINS))).astype(np.float32))
     labels = np.zeros((B, OCT), np.float32)
     labels[: B // 2, 3] = 1.0
     feat[: B // 2, :, 3 * 64 + 20] += 4.0      # a feature the positives carry
@@ -106,3 +131,39 @@ def test_training_reduces_loss_on_fixed_batch():
     assert last < 0.5 * first
     logits = net.forward(feat)
     assert (logits[: B // 2, 3].min() > logits[B // 2:, 3].max()).item()
+
+
+@pytest.mark.gpu
+def test_shipped_network_gains_over_selection_without_it():
+    """The shipped model on observations it never saw (seeds 20000+): recall
+    of the injections the exhaustive search detects, for the same window
+    budgets spent by an untrained network and by random choice.  The trained
+    network must recall more over the fraction sweep and find every detected
+    injection at its shipped fraction.  The max-coarse-S/N heuristic is
+    printed beside it."""
+    import torch
+    from gaffa_b200 import configs, proposal
+    cfg = configs.survey_size(nsamples=1 << 20)
+    dm_max = cfg.dm_low + (cfg.ndm - 1) * cfg.dm_step
+    examples, _, _ = proposal.make_examples(cfg, range(20_000, 20_006))
+    net = proposal.ProposalNet()
+    meta = net.load_default()
+    untrained = proposal.ProposalNet(seed=0)
+    rng = np.random.default_rng(0)
+    fractions = [k / proposal.NCOARSE for k in range(4, proposal.NCOARSE + 1, 4)]
+    curves = {
+        "trained": proposal.evaluate(lambda e: net.forward(e.features), examples, fractions, dm_max),
+        "untrained": proposal.evaluate(lambda e: untrained.forward(e.features), examples, fractions, dm_max),
+        "random": proposal.evaluate(lambda e: torch.from_numpy(rng.random((proposal.NCOARSE, 1))), examples,
+                                    fractions, dm_max),
+        "heuristic": proposal.evaluate(lambda e: proposal.baseline_scores(e.features), examples, fractions, dm_max),
+    }
+    total = curves["trained"][fractions[0]][1]
+    assert total >= 8
+    mean = {k: float(np.mean([v[f][0] / total for f in fractions])) for k, v in curves.items()}
+    print({k: round(v, 3) for k, v in mean.items()})
+    assert mean["trained"] > mean["untrained"] + 0.05
+    assert mean["trained"] > mean["random"] + 0.05
+    found, tot = proposal.evaluate(lambda e: net.forward(e.features), examples, [meta["fraction"]],
+                                   dm_max)[meta["fraction"]]
+    assert found == tot
