@@ -91,7 +91,7 @@ class Autotuner:
     DM step, log2 length) in memory and, given a path, in a JSON file.  All
     shapes give the same sums; only the speed differs."""
 
-    SHAPES = ((8, 64), (8, 32), (4, 64), (4, 32), (2, 64), (8, 16))
+    SHAPES = ((8, 64), (8, 32), (8, 16), (4, 32), (4, 16), (2, 16))
 
     def __init__(self, path: str | Path | None = None, dms: int = 64, repeats: int = 3):
         self.path = Path(path) if path else None

@@ -70,7 +70,7 @@ class DmSearch:
                  algorithm: str = "brute", subband_channels: int = 32, ndm_per_nominal: int = 32,
                  frequency_cluster_radius: float = 0.1, dm_cluster_radius: int = 1, fold_nbin: int = 64,
                  dm_batch: int | None = None, memory_budget: int | None = None, device_id: int = 0,
-                 harmonic_options=None):
+                 harmonic_options=None, launch_shape: tuple[int, int] | None = None):
         self.device = torch.device("cuda", device_id)
         freq = np.asarray(frequency_mhz, dtype=np.float64)
         self.frequency_low_mhz, self.frequency_high_mhz = float(freq.min()), float(freq.max())
@@ -83,7 +83,8 @@ class DmSearch:
         self.fold_nbin = fold_nbin
         self.dedisp = core.DedispersionProgram(frequency_mhz, nsamples, tsamp, dm_low, dm_step, ndm, nbits=nbits,
                                                algorithm=algorithm, subband_channels=subband_channels,
-                                               ndm_per_nominal=ndm_per_nominal, device_id=device_id)
+                                               ndm_per_nominal=ndm_per_nominal, device_id=device_id,
+                                               launch_shape=launch_shape if algorithm == "brute" else None)
         self.nout = self.dedisp.nout
         plan = core.make_riptide_ffa_plan(self.nout, tsamp, period_min, period_max, bins_min=bins_min,
                                           bins_max=bins_max, duty_cycle_max=duty_cycle_max)
