@@ -206,8 +206,10 @@ def _assert_same_result(a, b):
     if a.fold_profile is None:
         assert b.fold_profile is None
     else:
-        assert np.array_equal(np.asarray(a.fold_profile), np.asarray(b.fold_profile))
-        assert np.array_equal(np.asarray(a.fold_exposure), np.asarray(b.fold_exposure))
+        # the fold's FP64 sums are combined by shared-memory atomics, in a
+        # run-dependent order (the parity tests' fold tolerance)
+        np.testing.assert_allclose(np.asarray(a.fold_profile), np.asarray(b.fold_profile), rtol=1e-6)
+        np.testing.assert_allclose(np.asarray(a.fold_exposure), np.asarray(b.fold_exposure), rtol=1e-12)
 
 
 @pytest.mark.gpu
