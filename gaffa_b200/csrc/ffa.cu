@@ -43,7 +43,12 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kMaxBins = 512;
 constexpr int kMaxWidths = 64;
-constexpr int kClusterSize = 8;
+// Largest thread-block cluster for one (series, task).  One CTA per item:
+// on the survey plan at 16 and 256 series, clusters of up to 8 CTAs (sized
+// by rows) ran 11-15 % slower than independent CTAs, which need no cluster
+// barriers and keep every SM busy with its own item (16-CTA clusters were
+// slower still).
+constexpr int kClusterSize = 1;
 constexpr int kPrepareChunk = 16384;
 
 struct TaskDev {
@@ -717,6 +722,7 @@ using namespace gf;
 // rows per buffer, column-block sizes and the dynamic shared memory.
 struct FfaGeometry {
   uint32_t pitch = 0, max_rows = 0, block_rows = 0, final_rows = 0, levels = 0, front = 0;
+  uint32_t cp_rows = 0;        // root rows whose prefix sums fit one row buffer
   size_t smem_bytes = 0;
 };
 
@@ -856,12 +862,12 @@ void build_subtree_schedule(uint32_t n, std::vector<MetaEntry>& out) {
   }
 }
 
-// Pass boundaries: depth cuts from split_depth down to 0; the first pass
-// takes split_depth mod K levels (when non-zero), the others K levels.
-uint32_t cut_after(uint32_t d, uint32_t dS, uint32_t K) {
-  const uint32_t r = dS % K;
-  if (d == dS && r != 0) return dS - r;
-  return d >= K ? d - K : 0;
+// Pass boundaries: depth cuts from split_depth down to 0, K levels per pass;
+// the final pass takes the remainder (split_depth mod K, when non-zero).  A
+// final pass of fewer levels has a shallower cone, so its blocks hold more
+// root rows, and more threads share the sequential prefix sums of detection.
+uint32_t cut_after(uint32_t d, uint32_t K) {
+  return d > K ? d - K : 0;
 }
 
 // IEEE single arithmetic of ffa.cpp:153-171 (host code is built without
@@ -941,10 +947,13 @@ void build_task_passes(gf_ffa_program& P, const FfaGeometry& g, TaskDev& d) {
   d.pass_begin = static_cast<uint32_t>(P.passes.size());
   uint32_t depth = dS;
   while (true) {
-    const uint32_t dn = cut_after(depth, dS, K);
+    const uint32_t dn = cut_after(depth, K);
     const uint32_t levels = depth - dn;
     const bool final_pass = dn == 0;
-    const uint32_t R = final_pass ? g.final_rows : g.block_rows;
+    // final blocks: the rows whose cone of `levels` levels fits a row buffer
+    // (R + 3 (2^levels - 1) at the bottom) and whose prefix sums fit the other
+    const uint32_t R =
+        final_pass ? std::min<uint32_t>(g.max_rows - 3 * ((1u << levels) - 1), g.cp_rows) : g.block_rows;
     const uint32_t nnodes = 1u << dn;
     const uint32_t maxn = (d.rows + nnodes - 1) >> dn;
     const uint32_t limit = final_pass ? d.rows_eval : maxn;
@@ -1071,7 +1080,8 @@ std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& spe
     while (g.levels > 1 && static_cast<int>(rows) - 3 * ((1 << g.levels) - 1) < 8) --g.levels;
     g.block_rows = rows - 3 * ((1u << g.levels) - 1);
     const uint32_t cp_pitch = (cap + P->max_width + 2) | 1u;
-    g.final_rows = std::min<uint32_t>(g.block_rows, (rows * g.pitch) / cp_pitch);
+    g.cp_rows = (rows * g.pitch) / cp_pitch;
+    g.final_rows = std::min<uint32_t>(g.block_rows, g.cp_rows);
     check_arg(g.final_rows >= 1 && g.block_rows >= 1, "FFA bins too large for the shared-memory tiles");
     g.smem_bytes = smem_for(rows);
     max_rows_all = std::max(max_rows_all, rows);
