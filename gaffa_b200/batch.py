@@ -18,9 +18,11 @@ the pieces are packed into waves that fit the series arena.  Each wave runs
 captured once into a CUDA graph and replayed on later runs.  The dedispersion
 launch shapes (DMs per CTA, channel rows per staging step) come from an
 autotuner that times candidate shapes on the observation's own data and
-caches the winners by geometry.  Every result is identical to searching each
-observation with its own search.DmSearch: the kernels and the arithmetic are
-the same, only the launch grouping differs.
+caches the winners by geometry.  Peaks, candidates and harmonic flags are
+identical to searching each observation with its own search.DmSearch (the
+kernels and the arithmetic are the same, only the launch grouping differs);
+the fold of the top candidate agrees to the fold's own tolerance (its FP64
+sums are combined by atomics in a run-dependent order).
 """
 from __future__ import annotations
 
@@ -35,20 +37,6 @@ import torch
 
 from . import _lib, core
 from .search import SearchResult
-
-
-def prepared_floats(plan: core.FfaPlan) -> int:
-    """Floats of one prepared series: every distinct downsample factor's
-    prepared samples, each rounded up to 4 (the FFA program's layout)."""
-    seen = set()
-    off = 0
-    for t in plan.tasks:
-        f = float(t["downsample_factor"])
-        if f in seen:
-            continue
-        seen.add(f)
-        off = (off + int(t["prepared_nsamples"]) + 3) // 4 * 4
-    return (off + 3) // 4 * 4
 
 
 @dataclasses.dataclass
@@ -190,7 +178,7 @@ class BatchSearch:
                 plan = plan.with_widths(c.width_trials)
             self.plans.append(plan)
             self.strides.append((dd.nout + 3) // 4 * 4)
-            self.prep.append(prepared_floats(plan))
+            self.prep.append(plan.prepared_floats)
         self._tuned = False
         per_dm = [4 * (s + p) for s, p in zip(self.strides, self.prep)]
         if wave_bytes is None:

@@ -55,6 +55,19 @@ class FfaPlan:
     def nsamples(self) -> int:
         return int(self.tasks[0]["input_nsamples"]) if len(self.tasks) else 0
 
+    @property
+    def prepared_floats(self) -> int:
+        """Floats of one prepared series: every distinct downsample factor's
+        samples, each rounded up to 4 (the FFA program's layout), known
+        before any program exists."""
+        seen, off = set(), 0
+        for t in self.tasks:
+            f = float(t["downsample_factor"])
+            if f not in seen:
+                seen.add(f)
+                off = (off + int(t["prepared_nsamples"]) + 3) // 4 * 4
+        return off
+
     def with_widths(self, widths) -> "FfaPlan":
         return FfaPlan(self.tasks, widths)
 

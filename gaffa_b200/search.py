@@ -95,7 +95,7 @@ class DmSearch:
         g = self.dedisp.batch_granularity
         if dm_batch is None:
             free = torch.cuda.mem_get_info(self.device)[0] if memory_budget is None else memory_budget
-            per_dm = self.out_stride * 4 + self._prepared_floats_estimate() * 4
+            per_dm = self.out_stride * 4 + plan.prepared_floats * 4
             budget = int(free * 0.45) - self.dedisp.info.staged_bytes - (1 << 30)
             dm_batch = max(g, min(ndm, budget // max(1, per_dm)))
         dm_batch = max(g, (dm_batch // g) * g)
@@ -111,11 +111,6 @@ class DmSearch:
         if algorithm == "subband":
             self._workspace = torch.empty(self.dedisp.workspace_bytes(self.dm_batch), dtype=torch.uint8,
                                           device=self.device)
-
-    def _prepared_floats_estimate(self) -> int:
-        # upper bound used before the FFA program exists: sum over octaves of
-        # nout / factor is below nout for factors > 1
-        return self.nout + 64
 
     def stage(self, filterbank) -> torch.Tensor:
         return self.dedisp.stage(filterbank)

@@ -162,7 +162,6 @@ def _records_key(rec, task_offset=0):
 def test_ffa_batch_matches_one_program_per_plan():
     torch = _cuda()
     from gaffa_b200 import core
-    from gaffa_b200.batch import prepared_floats
     gen = torch.Generator(device="cuda").manual_seed(5)
     specs = [(40_000, 64e-6, 0.05, 1.0, 3), (131_072, 64e-6, 0.2, 4.0, 5), (70_001, 128e-6, 0.5, 4.0, 2)]
     plans, series = [], []
@@ -176,14 +175,14 @@ def test_ffa_batch_matches_one_program_per_plan():
         st[:, 1] = 1.0
         stats.append(st)
         batch.prepare(m, s, st)
-        assert batch.member_info[m].prepared_floats == prepared_floats(pl)
+        assert batch.member_info[m].prepared_floats == pl.prepared_floats
     batch.search_async(3.0)
     got = batch.collect(3.0)
     assert len(got) > 0
     want = []
     for m, (pl, s, st) in enumerate(zip(plans, series, stats)):
         prog = core.FfaProgram(pl, max_series=s.shape[0])
-        assert prog.prepared_floats == prepared_floats(pl)
+        assert prog.prepared_floats == pl.prepared_floats
         prep = prog.prepare(s, s.shape[0], st)
         mi = batch.member_info[m]
         want += _records_key(prog.search(prep, s.shape[0], 3.0), int(mi.task_begin))
