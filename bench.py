@@ -263,18 +263,26 @@ def proposal_measurement(cfg, ds, raw, exhaustive, fraction):
             "model_val_recall_at_fraction": meta.get("val_recall_at_fraction")}
 
 
-def batched_measurement(nobs: int, device_id: int) -> dict:
-    """The batched uneven workload at reduced size: nobs observations with the
-    batched laws (channels from {1024, 2048, 4096}, lengths log-uniform over
-    2^18-2^20, 256-1024 DM trials over 0-1000, own FFA period ranges).  Times
-    one batched run (one dedispersion launch and one FFA launch per class per
-    wave, replayed from captured CUDA graphs, autotuned dedispersion shapes)
-    against the same observations searched one after another by DmSearch,
-    both from HBM-resident filterbanks, and checks that the peaks agree."""
+BATCHED_CASES = {
+    # the batched laws at reduced lengths and DM counts
+    "reduced": dict(log2_nsamples=(18.0, 20.0), ndm_range=(256, 1024)),
+    # many small observations, where launches and host round trips dominate
+    "small": dict(nchans_choices=(256, 512, 1024), log2_nsamples=(16.0, 18.0), ndm_range=(64, 256)),
+}
+
+
+def batched_measurement(nobs: int, device_id: int, case: str = "reduced") -> dict:
+    """A batched uneven workload (BATCHED_CASES: the batched laws, channels
+    from {1024, 2048, 4096} or smaller, own FFA period ranges, 0-4 pulsars).
+    Times one batched run (one dedispersion launch and one FFA launch per
+    class per wave, replayed from captured CUDA graphs, autotuned
+    dedispersion shapes) against the same observations searched one after
+    another by DmSearch, both from HBM-resident filterbanks, and checks that
+    the peaks and candidates agree."""
     import numpy as np
     import torch
     from gaffa_b200 import batch, configs, core, search
-    cs = configs.batched_uneven(seed=0, nobs=nobs, log2_nsamples=(18.0, 20.0), ndm_range=(256, 1024))
+    cs = configs.batched_uneven(seed=0, nobs=nobs, **BATCHED_CASES[case])
     data = [core.synth_generate(c.obs, device_id=device_id) for c in cs]
     tuner = batch.Autotuner()
     t0 = time.perf_counter()
@@ -307,8 +315,7 @@ def batched_measurement(nobs: int, device_id: int) -> dict:
             "kernel_launches_per_run": launches, "seconds": sec_b, "seconds_staged_data": sec_replay,
             "sequential_value": units / sec_s, "sequential_seconds": sec_s, "speedup_vs_sequential": sec_s / sec_b,
             "identical_to_sequential": bool(same), "setup_seconds": setup,
-            "tuned_dedispersion_shapes": tuner.cache,
-            "config": "batched uneven laws at 2^18-2^20 samples and 256-1024 DM trials"}
+            "tuned_dedispersion_shapes": tuner.cache, "case": case, "laws": BATCHED_CASES[case]}
 
 
 def cpu_baseline(cfg, host_input, seconds: float) -> dict:
@@ -363,9 +370,10 @@ def main():
     from gaffa_b200 import core, search
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    batched = None
+    batched = batched_small = None
     if rank == 0 and world == 1 and not args.no_batched:
-        batched = batched_measurement(args.batched_observations, local)
+        batched = batched_measurement(args.batched_observations, local, "reduced")
+        batched_small = batched_measurement(64, local, "small")
     cfg = workload(args, rank)
     obs = cfg.obs
     raw = core.synth_generate(obs, device_id=local)          # device-resident filterbank
@@ -479,6 +487,7 @@ def main():
             "cpu_baseline": baseline,
             "proposal": prop,
             "batched": batched,
+            "batched_small": batched_small,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
