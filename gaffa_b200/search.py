@@ -168,11 +168,68 @@ class DmSearch:
 
     def run(self, filterbank, observation_seconds: float | None = None, timers: dict | None = None,
             dm_ranges=None) -> SearchResult:
-        t = {}
         t0 = time.perf_counter()
         with _StageTimer(timers, "stage"):
             staged = self.stage(filterbank)
         torch.cuda.synchronize(self.device)
+        return self._search(staged, t0, observation_seconds, timers, dm_ranges)
+
+    def run_many(self, filterbanks, observation_seconds: float | None = None) -> list:
+        """Searches observations one after another (host arrays or pinned host
+        tensors, time-major).  A helper thread stages observation i + 1 into a
+        second staging buffer (host-to-device copies and the transpose, on a
+        side stream) while observation i is searched, so the copies hide behind
+        the search.  Results equal run() of each observation."""
+        import threading
+        filterbanks = list(filterbanks)
+        n = len(filterbanks)
+        bufs = [torch.empty(int(self.dedisp.info.staged_bytes), dtype=torch.uint8, device=self.device)
+                for _ in range(min(2, n))]
+        side = torch.cuda.Stream(self.device)
+        ready = [threading.Event() for _ in range(n)]
+        freed = [threading.Event() for _ in range(n)]
+        errors = []
+
+        def stage_all():
+            try:
+                torch.cuda.set_device(self.device)
+                for i, fb in enumerate(filterbanks):
+                    if i >= 2:
+                        freed[i - 2].wait()
+                        if errors:
+                            return
+                    with torch.cuda.stream(side):
+                        self.dedisp.stage(fb, stream=side, out=bufs[i % 2])
+                    side.synchronize()
+                    ready[i].set()
+            except Exception as exc:  # re-raised on the searching thread
+                errors.append(exc)
+                for e in ready:
+                    e.set()
+
+        worker = threading.Thread(target=stage_all, daemon=True)
+        worker.start()
+        results = []
+        try:
+            for i in range(n):
+                t0 = time.perf_counter()
+                ready[i].wait()
+                if errors:
+                    raise errors[0]
+                results.append(self._search(bufs[i % 2], t0, observation_seconds, None, None))
+                torch.cuda.synchronize(self.device)
+                freed[i].set()
+        finally:
+            if len(results) < n:
+                # stop the helper before it stages into a buffer still in use
+                errors.append(RuntimeError("search stopped"))
+                for e in freed:
+                    e.set()
+            worker.join()
+        return results
+
+    def _search(self, staged: torch.Tensor, t0: float, observation_seconds, timers, dm_ranges) -> SearchResult:
+        t = {}
         t1 = time.perf_counter()
         peaks, launches = self.search_staged(staged, timers, dm_ranges)
         t2 = time.perf_counter()

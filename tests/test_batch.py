@@ -256,3 +256,22 @@ def test_batch_search_peak_buffer_growth_and_eager_mode():
     plain = batch.BatchSearch(cs, use_graphs=False).run(data)
     for a, b in zip(plain, want):
         _assert_same_result(a, b)
+
+
+@pytest.mark.gpu
+def test_run_many_overlaps_staging_and_matches_run():
+    """DmSearch.run_many stages observation i + 1 on a helper thread and side
+    stream while observation i is searched; every result equals run()."""
+    _cuda()
+    import dataclasses
+    from gaffa_b200 import search, synth
+    c = small_batch(1, seed=5)[0]
+    c.snr_threshold = 6.0
+    hosts = [synth.generate(dataclasses.replace(c.obs, seed=c.obs.seed + k)) for k in range(3)]
+    ds = search.from_config(c)
+    want = [ds.run(h) for h in hosts]
+    got = ds.run_many(hosts)
+    assert len(got) == 3
+    for a, b in zip(got, want):
+        _assert_same_result(a, b)
+    assert sum(len(r.peaks) for r in got) > 0
