@@ -620,6 +620,7 @@ __global__ void __launch_bounds__(kThreads, 2) ffa_search_kernel(SearchParams p)
         cp_async_wait_all();
         __syncthreads();
         detect_rows<NB>(buf0, pitch, 1, 0, buf1, cp_pitch, da);
+        __syncthreads();  // the width scans read buf1 until here; the next item loads into it
         continue;
       }
       float* lvl1 = eval_subtree<NB>(p, input, t.rows, bins, 1, buf0, buf1, cmeta);
@@ -633,6 +634,7 @@ __global__ void __launch_bounds__(kThreads, 2) ffa_search_kernel(SearchParams p)
         __syncthreads();
         detect_rows<NB>(other, pitch, cnt, b0, other + batch * pitch, cp_pitch, da);
       }
+      __syncthreads();  // the last width scans read `other` until here; the next item loads into it
       continue;
     }
     // 1. subtrees at depth dS, on chip, into scratch q0
@@ -661,6 +663,7 @@ __global__ void __launch_bounds__(kThreads, 2) ffa_search_kernel(SearchParams p)
         eval_block<NB>(p, hb, src, bins, buf0, buf1, cmeta);
         if (hb.final_pass) {
           detect_rows<NB>(buf0, pitch, hb.count[0], hb.out_row, buf1, cp_pitch, da);
+          __syncthreads();  // the width scans read buf1 until here; the next block may load into it
         } else {
           store_rows<NB>(buf0, pitch, hb.count[0], bins, dst + static_cast<uint64_t>(hb.out_row) * bins);
           __syncthreads();
