@@ -152,6 +152,20 @@ def test_degenerate_subband_equals_multi_dm(port, sbc):
                                   port.dedisperse_subband(data, freq, 2.0, 3.5, 17, 1500.0, 1e-3, sbc, npn))
 
 
+def test_single_dm_is_a_prefix_of_the_multi_dm_row(port):
+    # test_dedispersion.cpp:435-497: one DM's own series (its aligned spectrum
+    # summed over channels, valid over its own delay) starts with that DM's
+    # row of the multi-DM block (valid over the highest DM's delay)
+    rng = np.random.default_rng(7)
+    data = rng.integers(0, 256, (4000, 32), dtype=np.uint8)
+    freq = np.linspace(1500.0, 1200.0, 32)
+    multi = port.dedisperse_multi_dm(data, freq, 0.0, 4.0, 12, 1500.0, 1e-3)
+    for i in (0, 5, 11):
+        single = port.dedisperse_spectrum(data, freq, 4.0 * i, 1500.0, 1e-3).astype(np.uint32).sum(axis=1)
+        assert len(single) >= multi.shape[1]
+        assert np.array_equal(single[: multi.shape[1]], multi[i])
+
+
 def _riptide_snr(bins, width, boxsum, total, stdnoise):
     # test_ffa_detection.cpp:24-33 expected_riptide_snr (float arithmetic)
     b, w = np.float32(bins), np.float32(width)
