@@ -37,3 +37,50 @@ def test_c_program_builds_plan_and_reports_errors(tmp_path):
         assert float(factor) == float(t["downsample_factor"])
     err = re.search(r"error (-?\d+) (.*)", out.stdout)
     assert int(err.group(1)) == _lib.GF_EINVAL and "factor" in err.group(2)
+
+
+LAYOUTS = {
+    # C struct -> ctypes structure or numpy record dtype of gaffa_b200/_lib.py
+    "gf_ffa_task": ("FfaTask", "TASK_DTYPE"), "gf_plan_options": ("PlanOptions",),
+    "gf_dedisp_desc": ("DedispDesc",), "gf_dedisp_info": ("DedispInfo",),
+    "gf_dedisp_batch_item": ("DedispBatchItem",), "gf_filterbank_header": ("FilterbankHeader",),
+    "gf_preprocess_desc": ("PreprocessDesc",), "gf_preprocess_info": ("PreprocessInfo",),
+    "gf_ffa_info": ("FfaInfo",), "gf_ffa_batch_member": ("FfaBatchMember",),
+    "gf_ffa_member_info": ("FfaMemberInfo",), "gf_peak_record": ("PEAK_RECORD_DTYPE",),
+    "gf_peak": ("PEAK_DTYPE",), "gf_candidate_options": ("CandidateOptions",), "gf_candidate": ("CAND_DTYPE",),
+    "gf_harmonic_context": ("HarmonicContext",), "gf_harmonic_options": ("HarmonicOptions",),
+    "gf_harmonic_relation": ("HARMONIC_DTYPE",), "gf_synth_pulsar": ("SynthPulsar",),
+    "gf_synth_desc": ("SynthDesc",),
+}
+
+
+def test_binding_struct_layouts_match_the_header(tmp_path):
+    """Every POD struct of include/gaffa_b200.h has the size and field offsets
+    that the ctypes / numpy declarations of the Python binding assume."""
+    import ctypes as C
+    from gaffa_b200 import _lib
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not found")
+    want, lines = [], []
+    for cname, pynames in LAYOUTS.items():
+        for pyname in pynames:
+            obj = getattr(_lib, pyname)
+            if isinstance(obj, type) and issubclass(obj, C.Structure):
+                fields = [(f[0], getattr(obj, f[0]).offset) for f in obj._fields_]
+                size = C.sizeof(obj)
+            else:
+                fields = [(n, obj.fields[n][1]) for n in obj.names]
+                size = obj.itemsize
+            lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+            want.append(f"{cname} size {size}")
+            for name, off in fields:
+                lines.append(f'  printf("{cname}.{name} %zu\\n", offsetof({cname}, {name}));')
+                want.append(f"{cname}.{name} {off}")
+    src = tmp_path / "layouts.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "gaffa_b200.h"\nint main(void) {\n' +
+                   "\n".join(lines) + "\n  return 0;\n}\n")
+    exe = tmp_path / "layouts"
+    subprocess.run([gcc, "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    assert [g for g in got if g] == want
