@@ -93,3 +93,20 @@ def test_host_noise_model_moments():
     counts = np.bincount(lv.reshape(-1), minlength=4) / lv.size
     assert np.all(np.abs(counts - 0.25) < 0.01)
     assert np.array_equal(synth.unpack_2bit(synth.pack_2bit(lv), 64), lv)
+
+
+def test_binding_argument_counts_match_the_prototypes(lib):
+    """Each ctypes signature of gaffa_b200/_lib.py takes as many arguments as
+    the header's prototype (a missing or extra argument would shift every
+    later one on the stack)."""
+    text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "gaffa_b200.h").read_text(), flags=re.S)
+    protos = {}
+    for m in re.finditer(r"\b(gf_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text):
+        args = " ".join(m.group(2).split())
+        protos[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    checked = 0
+    for name, _res, argtypes in lib._SIGNATURES:
+        if name in protos:
+            assert len(argtypes) == protos[name], (name, len(argtypes), protos[name])
+            checked += 1
+    assert checked >= 0.9 * len(lib._SIGNATURES)
