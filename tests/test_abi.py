@@ -110,3 +110,27 @@ def test_binding_argument_counts_match_the_prototypes(lib):
             assert len(argtypes) == protos[name], (name, len(argtypes), protos[name])
             checked += 1
     assert checked >= 0.9 * len(lib._SIGNATURES)
+
+
+def test_binding_argument_types_match_the_prototypes(lib):
+    """Pointers are passed as pointers and scalars with the C scalar's width
+    and kind (a double where the C side reads a float, or a 32-bit integer
+    where it reads 64 bits, would be read wrongly without any error)."""
+    import ctypes as C
+    text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "gaffa_b200.h").read_text(), flags=re.S)
+    scalars = {"uint64_t": C.c_uint64, "int64_t": C.c_int64, "uint32_t": C.c_uint32, "int32_t": C.c_int32,
+               "int": C.c_int, "double": C.c_double, "float": C.c_float}
+    protos = {m.group(1): " ".join(m.group(2).split())
+              for m in re.finditer(r"\b(gf_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text)}
+    for name, _res, argtypes in lib._SIGNATURES:
+        args = protos[name]
+        params = [] if args in ("", "void") else [p.strip() for p in args.split(",")]
+        for p, t in zip(params, argtypes):
+            if "*" in p:
+                assert t is C.c_void_p or issubclass(t, (C._Pointer, C.Array, C.c_char_p)), (name, p, t)
+            else:
+                base = p.replace("const ", "").split()[0]
+                assert base in scalars, (name, p)
+                want = scalars[base]
+                assert C.sizeof(t) == C.sizeof(want) and (t in (C.c_float, C.c_double)) == (
+                    want in (C.c_float, C.c_double)), (name, p, t)
