@@ -37,9 +37,9 @@ METRIC = "DM-trial·samples/s searched"
 UNIT = "DM-trial·samples/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes (read + write) one FFA search moves per DM-trial series, from the
-# ncu capture summarised in this file (survey-size workload only)
-FFA_TRAFFIC_FILE = ROOT / "profiles" / "ffa_search_kernel_survey_size.md"
+# DRAM bytes (read + write) one FFA search moves per DM-trial series, from an
+# ncu capture of the survey-size FFA plan (recorded with its command)
+FFA_TRAFFIC_FILE = ROOT / "profiles" / "ffa_search_kernel_survey_size.json"
 
 
 def parse_args():
@@ -132,16 +132,13 @@ class ClockSampler:
 
 
 def ffa_traffic_per_series(workload: str):
-    """traffic_bytes_per_series recorded in the FFA profile summary."""
+    """traffic_bytes_per_series of the recorded FFA capture (survey size only)."""
     if workload != "survey_size":
         return None
     try:
-        for line in FFA_TRAFFIC_FILE.read_text().splitlines():
-            if line.strip().startswith("traffic_bytes_per_series:"):
-                return float(line.split(":", 1)[1])
-    except OSError:
-        pass
-    return None
+        return float(json.loads(FFA_TRAFFIC_FILE.read_text())["traffic_bytes_per_series"])
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 def measured_hbm_gbs():
@@ -433,7 +430,7 @@ def main():
                 "traffic": traffic, "kernel": dominant, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_ms,
                 "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in totals.items()}}
-    # the compute roofs that actually bind these kernels
+    # the compute roofs that bind these kernels: byte adds and FFA element-levels
     if "ffa" in totals:
         per_series = float(sum(int(t["rows"]) * int(t["bins"]) * max(1, int(t["rows"]) - 1).bit_length()
                                for t in ds.plan.tasks))

@@ -167,7 +167,9 @@ void* g_fold_scratch_address[kMaxDevices] = {};
 
 // Device address of g_fold_scratch on the current device, resolved once per
 // device.  In host code the array's name is only a host-side stand-in, so
-// the kernels must receive this address, never &g_fold_scratch.
+// the kernels must receive this address, never &g_fold_scratch.  The address
+// is kept for the life of the process; a cudaDeviceReset reloads the module
+// and makes it stale, so the entry point is not to be used after a reset.
 void* fold_scratch_address() {
   int device = -1;
   cuda_check(cudaGetDevice(&device), "cudaGetDevice");
@@ -191,22 +193,25 @@ extern "C" int gf_fold_time_series_noalloc(const void* dev_input, int32_t input_
   return guarded([&] {
     check_arg(n > 0, "fold input must not be empty");
     check_arg(nbin > 0, "fold nbin must be positive");
-    const uint64_t need = fold_blocks(n) * 2 * nbin * sizeof(double);
-    if (need > kNoAllocScratchBytes) {
+    check_arg(nbin <= kMaxBins, "CUDA fold supports nbin <= 8192");
+    const uint64_t nblocks = fold_blocks(n);
+    check_arg(nblocks < (1ull << 31), "fold input too long");
+    // each block keeps 2 * nbin doubles; compared by division so nothing wraps
+    if (nblocks > kNoAllocScratchBytes / (2 * nbin * sizeof(double))) {
       raise(GF_EINVAL, "fold without allocation: " + std::to_string(n) + " samples x " + std::to_string(nbin) +
-                           " bins need " + std::to_string(need) + " bytes of scratch, above the fixed " +
-                           std::to_string(kNoAllocScratchBytes) + " bytes; use gf_fold_time_series");
+                           " bins need " + std::to_string(nblocks) + " x " + std::to_string(2 * nbin * 8) +
+                           " bytes of scratch, above the fixed " + std::to_string(kNoAllocScratchBytes) +
+                           " bytes; use gf_fold_time_series");
     }
     // folding.cpp:44-73 validation, as gf_fold_time_series
     check_arg(std::isfinite(period) && period > 0.0, "fold period must be finite and positive");
     check_arg(std::isfinite(tsamp) && tsamp > 0.0, "fold tsamp must be finite and positive");
-    check_arg(nbin <= kMaxBins, "CUDA fold supports nbin <= 8192");
     check_arg(dev_input && dev_profile && dev_exposure && dev_status, "null argument");
     const double step = tsamp / period * static_cast<double>(nbin);
     const double hi = static_cast<double>(start_sample + n - 1) * step + step;
     check_arg(std::isfinite(hi) && std::ceil(hi) < 9.2e18, "fold phase bin index exceeds int64 range");
     auto s = as_stream(stream);
-    const uint64_t blocks = fold_blocks(n);
+    const uint64_t blocks = nblocks;
     double* partial = static_cast<double*>(fold_scratch_address());
     // the status word must start at zero; the partial sums are overwritten
     cuda_check(cudaMemsetAsync(dev_status, 0, 4, s), "cudaMemsetAsync(fold status)");

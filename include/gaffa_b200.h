@@ -609,8 +609,11 @@ int gf_fold_time_series(const void* dev_input, int32_t input_is_u32, uint64_t n,
  * requests fail with GF_EINVAL.  dev_status (caller-owned, uint32) receives
  * GF_STATUS_NONFINITE for non-finite float input.  The first call on a
  * device resolves the array's device address for that device (call it once
- * before any stream capture).  All calls share the array: calls that
- * overlap on the GPU race on it and must be serialised by the caller. */
+ * before any stream capture).  That address is kept for the life of the
+ * process: after a cudaDeviceReset the library's module is reloaded and the
+ * kept address is stale, so do not use this entry point after a reset.  All
+ * calls share the array: calls that overlap on the GPU race on it and must be
+ * serialised by the caller. */
 uint64_t gf_fold_noalloc_max_bytes(void);
 int gf_fold_time_series_noalloc(const void* dev_input, int32_t input_is_u32,
                                 uint64_t n, double period, double tsamp,

@@ -85,11 +85,12 @@ class OracleError(RuntimeError):
 
 
 def build(ref_dir: str | None = None) -> None:
-    """Compile the port and, when the reference sources exist, the reference."""
+    """Compile the port and, when ``ref_dir`` (or the GAFFA_REFERENCE_DIR
+    environment variable) names a gaffa checkout, the reference."""
     env = dict(os.environ)
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True, env=env)
-    ref = ref_dir or "/root/reference"
-    if Path(ref, "src", "gaffa").is_dir():
+    ref = ref_dir or os.environ.get("GAFFA_REFERENCE_DIR")
+    if ref and Path(ref, "src", "gaffa").is_dir():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_DIR={ref}"],
                        check=True, env=env)
 

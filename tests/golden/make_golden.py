@@ -21,6 +21,7 @@ Writes
 from __future__ import annotations
 
 import argparse
+import os
 import hashlib
 import sys
 import time
@@ -268,9 +269,11 @@ def filterbank_cases(ref: Oracle) -> dict:
 
 
 def ref_dir() -> str:
-    import re
-    make = (ROOT / "oracle" / "Makefile").read_text()
-    return re.search(r"^REF_DIR \?= (.+)$", make, re.M).group(1).strip()
+    """The gaffa checkout the fixtures come from (GAFFA_REFERENCE_DIR)."""
+    path = os.environ.get("GAFFA_REFERENCE_DIR")
+    if not path:
+        raise SystemExit("set GAFFA_REFERENCE_DIR to the gaffa checkout")
+    return path
 
 
 def main() -> None:
