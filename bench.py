@@ -19,6 +19,7 @@ host cores of rank 0.
 from __future__ import annotations
 
 import argparse
+import functools
 import json
 import os
 import statistics
@@ -53,7 +54,8 @@ def parse_args():
     ap.add_argument("--nsamples-log2", type=int, default=None, help="override the length (testing)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU baseline sample time")
+    ap.add_argument("--cpu-dms", type=int, default=8,
+                    help="DM trials in the CPU baseline sample (at least 5, the reference's parallel DM path)")
     ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal measurement")
     ap.add_argument("--proposal-fraction", type=float, default=None,
                     help="fraction of DM windows searched (default: the shipped model's)")
@@ -166,54 +168,147 @@ def algorithmic_bytes(stage: str, cfg, ds, units: int) -> float:
     return 0.0
 
 
-def run_reference(args, rank: int, world: int) -> None:
-    """Reference CPU implementation (oracle/_ref, else the port) on a bounded
-    DM-trial sample of the workload, with every host core."""
-    import torch
-    if rank != 0:
-        return
-    from oracle.oracle import Oracle
-    kind = "reference" if Oracle.available("reference") else "port"
-    ref = Oracle(kind)
-    cfg = workload(args)
-    obs = cfg.obs
-    from gaffa_b200 import core
-    data = core.synth_generate(obs).cpu().numpy()
-    freq = obs.frequencies
-    nout = ref.output_nsamples(freq, obs.nsamples, cfg.dm_low, cfg.dm_step, cfg.ndm, obs.ref_frequency, obs.tsamp)
-    cores = os.cpu_count() or 1
+def set_cpu_threads() -> None:
+    """OpenMP settings for the CPU legs (before any OpenMP runtime starts):
+    one thread per physical core, threads bound close, one place per core
+    (as the reference's own benchmark recipes run it)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(host_cpu()["physical_cores"]))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
 
-    def one_step(nsel):
-        idx = np.linspace(0, cfg.ndm - 1, nsel).round().astype(int)
+
+@functools.lru_cache(maxsize=None)
+def host_cpu() -> dict:
+    """The host's CPU model and core counts (the cores this process may use),
+    read once before any OpenMP runtime binds this thread to one core."""
+    logical = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        import psutil
+        physical = psutil.cpu_count(logical=False) or logical
+    except ImportError:
+        physical = logical
+    physical = max(1, min(physical, logical))
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"model": model, "physical_cores": physical, "logical_cpus": logical}
+
+
+class ReferenceCpuPath:
+    """The reference's own CPU implementation of the path (oracle/_ref: its
+    sources compiled where they lie; else the C restatement) on a contiguous
+    sample of DM trials at full length: dedisperse_multi_dm_cpu (or
+    dedisperse_subband_cpu on the unpacked 2-bit levels), find_dm_peaks_cpu
+    (convert, detrend, normalise, FFA, S/N), select_candidates_cpu and
+    fold_time_series_cpu of the best candidate -- the chain of
+    dm_search.cpp:142-199 and candidate.cpp:35-212."""
+
+    def __init__(self, cfg, data: np.ndarray):
+        from oracle.oracle import Oracle
+        self.kind = "reference" if Oracle.available("reference") else "port"
+        self.ref = Oracle(self.kind)
+        self.cfg = cfg
+        obs = cfg.obs
+        if obs.nbits == 2:
+            from gaffa_b200 import synth  # numpy only
+            data = synth.unpack_2bit(data, obs.nchans)   # the reference has no packed-input path
+        self.data = data
+        self.nout = self.ref.output_nsamples(obs.frequencies, obs.nsamples, cfg.dm_low, cfg.dm_step, cfg.ndm,
+                                             obs.ref_frequency, obs.tsamp)
+        self.widths = None if cfg.width_trials is None else np.array(cfg.width_trials, np.uint64)
+
+    def sample_size(self, minimum: int) -> int:
+        """DM trials per step: at least `minimum`, and for subband dedispersion
+        whole nominal-DM groups, so stage 1 is amortised as in a full run."""
+        cfg = self.cfg
+        n = minimum
+        if cfg.dedispersion == "subband":
+            g = cfg.ndm_per_nominal
+            n = max(g, (n + g - 1) // g * g)
+        return min(n, cfg.ndm)
+
+    def first_dm(self, nsel: int) -> int:
+        """A contiguous sample in the middle of the DM range (aligned to the
+        nominal-DM groups for subband dedispersion)."""
+        cfg = self.cfg
+        b0 = (cfg.ndm - nsel) // 2
+        if cfg.dedispersion == "subband":
+            b0 -= b0 % cfg.ndm_per_nominal
+        return max(0, b0)
+
+    def step(self, nsel: int) -> float:
+        cfg, obs, ref = self.cfg, self.cfg.obs, self.ref
+        b0 = self.first_dm(nsel)
+        dm0 = cfg.dm_low + b0 * cfg.dm_step
         t0 = time.perf_counter()
-        blocks = [ref.dedisperse_multi_dm(data, freq, cfg.dm_low + i * cfg.dm_step, cfg.dm_step, 1,
-                                          obs.ref_frequency, obs.tsamp)[:, :nout] for i in idx]
-        blk = np.ascontiguousarray(np.concatenate(blocks))
-        peaks = ref.find_dm_peaks(blk, cfg.dms[idx], obs.tsamp, cfg.plan_options(), cfg.preprocess_options(),
-                                  cfg.snr_threshold,
-                                  widths=None if cfg.width_trials is None else np.array(cfg.width_trials, np.uint64))
+        if cfg.dedispersion == "subband":
+            blk = ref.dedisperse_subband(self.data, obs.frequencies, dm0, cfg.dm_step, nsel, obs.ref_frequency,
+                                         obs.tsamp, subband_channels=cfg.subband_channels,
+                                         ndm_per_nominal=cfg.ndm_per_nominal)
+        else:
+            blk = ref.dedisperse_multi_dm(self.data, obs.frequencies, dm0, cfg.dm_step, nsel, obs.ref_frequency,
+                                          obs.tsamp)
+        blk = np.ascontiguousarray(blk[:, : self.nout])
+        peaks = ref.find_dm_peaks(blk, cfg.dms[b0:b0 + nsel], obs.tsamp, cfg.plan_options(),
+                                  cfg.preprocess_options(), cfg.snr_threshold, widths=self.widths)
         cands = ref.select_candidates(peaks, obs.nsamples * obs.tsamp)
         if len(cands):
-            ref.fold(blk[0], float(cands[0]["period"]), obs.tsamp, cfg.fold_nbin)
+            # DmPeak::dm_index indexes the rows of the searched block
+            ref.fold(blk[int(cands[0]["dm_index"])], float(cands[0]["period"]), obs.tsamp, cfg.fold_nbin)
         return time.perf_counter() - t0
 
-    # size the sample: a small probe, then scale to the target seconds
-    probe = max(1, min(cfg.ndm, 2 * cores // 8 or 1))
-    dt = one_step(probe)
-    nsel = int(max(1, min(cfg.ndm, probe * args.cpu_seconds / max(dt, 1e-3))))
-    for _ in range(max(0, args.warmup - 1)):
-        one_step(nsel)
-    times = [one_step(nsel) for _ in range(args.steps)]
+    def describe(self, nsel: int, seconds: float) -> str:
+        cfg = self.cfg
+        b0 = self.first_dm(nsel)
+        dd = "dedisperse_subband_cpu" if cfg.dedispersion == "subband" else "dedisperse_multi_dm_cpu"
+        return (f"DM trials {b0}-{b0 + nsel - 1} of {cfg.ndm} (contiguous), full length ({self.nout} samples): "
+                f"{dd} + find_dm_peaks_cpu + select_candidates_cpu + fold_time_series_cpu, {seconds:.1f} s; "
+                f"{os.environ.get('OMP_NUM_THREADS')} OpenMP threads, OMP_PROC_BIND="
+                f"{os.environ.get('OMP_PROC_BIND')}, OMP_PLACES={os.environ.get('OMP_PLACES')}")
+
+
+# find_dm_peaks_cpu runs its DM loop in parallel only for more than 4 trials
+# (dm_search.cpp:160), so every reference sample holds at least 5
+REFERENCE_MIN_DMS = 5
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    """Reference CPU implementation (oracle/_ref, else the port) on a bounded
+    DM-trial sample of the workload, with every physical host core.  The input
+    is the same seeded observation, generated on the host cores by the
+    checkers' generator (oracle/synth_oracle.c), so this arm never loads the
+    CUDA library."""
+    if rank != 0:
+        return
+    from oracle import oracle
+    cfg = workload(args)
+    obs = cfg.obs
+    cpu = host_cpu()
+    t0 = time.perf_counter()
+    data = oracle.synth_generate(obs)
+    gen_s = time.perf_counter() - t0
+    path = ReferenceCpuPath(cfg, data)
+    nsel = path.sample_size(REFERENCE_MIN_DMS)
+    # the CPU path has no device state or compilation to warm: one untimed
+    # step faults in the pages, then K timed steps
+    path.step(nsel)
+    times = [path.step(nsel) for _ in range(args.steps)]
     sec = sum(times) / len(times)
-    value = nsel * nout / sec
+    value = nsel * path.nout / sec
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
-        "config": {"workload": cfg.name, "nchans": obs.nchans, "nsamples": obs.nsamples, "ndm": cfg.ndm,
-                   "nout": nout, "dedispersion": cfg.dedispersion},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"{nsel} of {cfg.ndm} DM trials (evenly spaced), full length, per step"},
+        "config": {"workload": cfg.name, "nchans": obs.nchans, "nsamples": obs.nsamples, "nbits": obs.nbits,
+                   "ndm": cfg.ndm, "nout": path.nout, "dedispersion": cfg.dedispersion},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                         "kind": path.kind, "cpu": cpu,
+                         "sample": path.describe(nsel, sec) + f"; input generated in {gen_s:.1f} s (untimed)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -315,39 +410,19 @@ def batched_measurement(nobs: int, device_id: int, case: str = "reduced") -> dic
             "tuned_dedispersion_shapes": tuner.cache, "case": case, "laws": BATCHED_CASES[case]}
 
 
-def cpu_baseline(cfg, host_input, seconds: float) -> dict:
-    from oracle.oracle import Oracle
-    kind = "reference" if Oracle.available("reference") else "port"
-    ref = Oracle(kind)
-    obs = cfg.obs
-    freq = obs.frequencies
-    data = host_input
-    nout = ref.output_nsamples(freq, obs.nsamples, cfg.dm_low, cfg.dm_step, cfg.ndm, obs.ref_frequency, obs.tsamp)
-
-    def run(nsel):
-        idx = np.linspace(0, cfg.ndm - 1, nsel).round().astype(int)
-        t0 = time.perf_counter()
-        blocks = [ref.dedisperse_multi_dm(data, freq, cfg.dm_low + i * cfg.dm_step, cfg.dm_step, 1,
-                                          obs.ref_frequency, obs.tsamp)[:, :nout] for i in idx]
-        blk = np.ascontiguousarray(np.concatenate(blocks))
-        peaks = ref.find_dm_peaks(blk, cfg.dms[idx], obs.tsamp, cfg.plan_options(), cfg.preprocess_options(),
-                                  cfg.snr_threshold,
-                                  widths=None if cfg.width_trials is None else np.array(cfg.width_trials, np.uint64))
-        ref.select_candidates(peaks, obs.nsamples * obs.tsamp)
-        return time.perf_counter() - t0
-
-    cores = os.cpu_count() or 1
-    probe = max(1, min(cfg.ndm, cores // 4 or 1))
-    dt = run(probe)
-    nsel = int(max(1, min(cfg.ndm, probe * seconds / max(dt, 1e-3))))
-    dt = run(nsel) if nsel != probe else dt
-    return {"value": nsel * nout / dt, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{nsel} of {cfg.ndm} DM trials (evenly spaced), full length: dedisperse_multi_dm_cpu + "
-                      f"find_dm_peaks_cpu + select_candidates_cpu, {dt:.1f} s"}
+def cpu_baseline(cfg, host_input, min_dms: int) -> dict:
+    """The reference CPU path on a contiguous sample of at least `min_dms` DM
+    trials of the same observation (ReferenceCpuPath), timed once."""
+    path = ReferenceCpuPath(cfg, host_input)
+    nsel = path.sample_size(min_dms)
+    dt = path.step(nsel)
+    return {"value": nsel * path.nout / dt, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+            "kind": path.kind, "cpu": host_cpu(), "sample": path.describe(nsel, dt)}
 
 
 def main():
     args = parse_args()
+    set_cpu_threads()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
@@ -478,9 +553,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         src = host.numpy() if host is not None else raw.cpu().numpy()
         try:
-            baseline = cpu_baseline(cfg, src, args.cpu_seconds)
+            baseline = cpu_baseline(cfg, src, max(REFERENCE_MIN_DMS, args.cpu_dms))
         except Exception as exc:  # the baseline is reported, never the target
-            baseline = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            baseline = {"value": None, "unit": UNIT, "cores": host_cpu()["physical_cores"], "kind": "reference",
                         "sample": f"failed: {exc}"}
 
     if rank == 0:

@@ -262,6 +262,26 @@ int gfo_fold_time_series_u32(const uint32_t* in, uint64_t n, double period,
                              double tsamp, uint64_t nbin, uint64_t start_sample,
                              float* profile, double* exposure);
 
+/* ---- synthetic observations (synth_oracle.c; no reference counterpart) ---- */
+typedef struct {
+  double period, dm, duty_cycle, amplitude, phase;
+} gfo_synth_pulsar;
+
+typedef struct {
+  uint64_t nchans, nsamples;
+  double tsamp, f_low, f_high;
+  int32_t nbits, npulsars;
+  uint64_t seed;
+  const gfo_synth_pulsar* pulsars;
+  const uint8_t* narrowband_mask; /* nchans bytes, or NULL */
+  double narrowband_hz, narrowband_amplitude;
+  double impulse_hz, impulse_amplitude;
+} gfo_synth_desc;
+
+/* Rows [t_begin, t_end) of the gaffa_b200/synth.py observation, time-major:
+ * nchans bytes per row (8-bit) or nchans/4 packed bytes (2-bit). */
+int gfo_synth_generate(const gfo_synth_desc* d, uint64_t t_begin, uint64_t t_end, uint8_t* out);
+
 #ifdef __cplusplus
 }
 #endif

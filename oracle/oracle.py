@@ -386,3 +386,46 @@ def PORT_LIB_HANDLE():
         _PORT_HANDLE = C.CDLL(str(PORT_LIB))
         _PORT_HANDLE.gfo_last_error.restype = C.c_char_p
     return _PORT_HANDLE
+
+
+class _SynthPulsar(C.Structure):
+    _fields_ = [("period", C.c_double), ("dm", C.c_double), ("duty_cycle", C.c_double),
+                ("amplitude", C.c_double), ("phase", C.c_double)]
+
+
+class _SynthDesc(C.Structure):
+    _fields_ = [("nchans", C.c_uint64), ("nsamples", C.c_uint64), ("tsamp", C.c_double),
+                ("f_low", C.c_double), ("f_high", C.c_double), ("nbits", C.c_int32), ("npulsars", C.c_int32),
+                ("seed", C.c_uint64), ("pulsars", C.POINTER(_SynthPulsar)),
+                ("narrowband_mask", C.POINTER(C.c_uint8)), ("narrowband_hz", C.c_double),
+                ("narrowband_amplitude", C.c_double), ("impulse_hz", C.c_double),
+                ("impulse_amplitude", C.c_double)]
+
+
+def synth_generate(obs, t_begin: int = 0, t_end: int | None = None, out: np.ndarray | None = None) -> np.ndarray:
+    """Rows [t_begin, t_end) of a gaffa_b200.synth.Observation on the host
+    cores (synth_oracle.c): uint8 [time][channel], or packed 2-bit bytes
+    [time][channel/4] for 2-bit observations.  Same noise bits as the numpy
+    and CUDA generators; lets CPU-only callers build an input without the
+    CUDA library."""
+    from gaffa_b200 import synth  # numpy only: the channel mask
+    t_end = obs.nsamples if t_end is None else t_end
+    row = obs.nchans if obs.nbits == 8 else obs.nchans // 4
+    if out is None:
+        out = np.empty((t_end - t_begin, row), np.uint8)
+    if out.shape != (t_end - t_begin, row) or out.dtype != np.uint8 or not out.flags.c_contiguous:
+        raise ValueError("out must be a contiguous uint8 array of the requested rows")
+    ps = (_SynthPulsar * max(1, len(obs.pulsars)))()
+    for i, p in enumerate(obs.pulsars):
+        ps[i] = _SynthPulsar(p.period, p.dm, p.duty_cycle, p.amplitude, p.phase)
+    mask = None
+    if obs.rfi.narrowband_fraction > 0.0:
+        mask = np.ascontiguousarray(synth._narrowband_mask(obs).astype(np.uint8))
+    d = _SynthDesc(obs.nchans, obs.nsamples, obs.tsamp, obs.f_low, obs.f_high, obs.nbits, len(obs.pulsars),
+                   obs.seed, ps, None if mask is None else _ptr(mask, C.c_uint8), obs.rfi.narrowband_hz,
+                   obs.rfi.narrowband_amplitude, obs.rfi.impulse_hz, obs.rfi.impulse_amplitude)
+    rc = PORT_LIB_HANDLE().gfo_synth_generate(C.byref(d), C.c_uint64(t_begin), C.c_uint64(t_end),
+                                              out.ctypes.data_as(C.c_void_p))
+    if rc:
+        raise OracleError(rc, "gfo_synth_generate: invalid observation or rows")
+    return out
