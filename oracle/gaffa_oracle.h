@@ -262,6 +262,14 @@ int gfo_fold_time_series_u32(const uint32_t* in, uint64_t n, double period,
                              double tsamp, uint64_t nbin, uint64_t start_sample,
                              float* profile, double* exposure);
 
+/* ---- FP64 FFA search of one task (ffa64_oracle.c): the precision reference ---- */
+int gfo64_downsample(const float* in, uint64_t n, double factor, double* out, uint64_t* nout);
+int gfo64_ffa_transform(const double* in, uint64_t rows, uint64_t bins, double* out);
+/* S/N and first best phase for every evaluated row and width, no threshold:
+ * snr and phase are [rows_eval][nw]. */
+int gfo64_ffa_task_snr(const float* series, uint64_t n, const gfo_ffa_task* task, const uint64_t* widths,
+                       uint64_t nw, double* snr, uint64_t* phase);
+
 /* ---- synthetic observations (synth_oracle.c; no reference counterpart) ---- */
 typedef struct {
   double period, dm, duty_cycle, amplitude, phase;

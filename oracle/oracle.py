@@ -429,3 +429,31 @@ def synth_generate(obs, t_begin: int = 0, t_end: int | None = None, out: np.ndar
     if rc:
         raise OracleError(rc, "gfo_synth_generate: invalid observation or rows")
     return out
+
+
+def ffa64_task_snr(series: np.ndarray, task, widths) -> tuple[np.ndarray, np.ndarray]:
+    """FP64 S/N and first best phase, [rows_eval][len(widths)], of one plan task
+    (TASK_DTYPE record) on a normalised float series (ffa64_oracle.c)."""
+    series = np.ascontiguousarray(series, np.float32)
+    widths = np.ascontiguousarray(widths, np.uint64)
+    t = np.ascontiguousarray(np.array(task, TASK_DTYPE).reshape(1))
+    re, nw = int(t["rows_eval"][0]), len(widths)
+    snr = np.zeros((re, nw), np.float64)
+    phase = np.zeros((re, nw), np.uint64)
+    rc = PORT_LIB_HANDLE().gfo64_ffa_task_snr(
+        _ptr(series, C.c_float), C.c_uint64(len(series)), t.ctypes.data_as(C.c_void_p),
+        _ptr(widths, C.c_uint64), C.c_uint64(nw), _ptr(snr, C.c_double), _ptr(phase, C.c_uint64))
+    if rc:
+        raise OracleError(rc, "gfo64_ffa_task_snr: invalid task, widths or series")
+    return snr, phase
+
+
+def ffa64_transform(x: np.ndarray, bins: int) -> np.ndarray:
+    """FP64 FFA transform of a [rows][bins] block (ffa64_oracle.c)."""
+    x = np.ascontiguousarray(x, np.float64).reshape(-1, bins)
+    out = np.zeros_like(x)
+    rc = PORT_LIB_HANDLE().gfo64_ffa_transform(_ptr(x, C.c_double), C.c_uint64(x.shape[0]), C.c_uint64(bins),
+                                               _ptr(out, C.c_double))
+    if rc:
+        raise OracleError(rc, "gfo64_ffa_transform: invalid shape")
+    return out

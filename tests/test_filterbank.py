@@ -17,10 +17,10 @@ GOLDEN = Path(__file__).resolve().parent / "golden" / "ref_filterbank.npz"
 
 
 def _reference_fil() -> Path:
-    """basetest.fil under the reference checkout the oracle recipe builds from."""
-    import re
-    make = (Path(__file__).resolve().parents[1] / "oracle" / "Makefile").read_text()
-    return Path(re.search(r"^REF_DIR \?= (.+)$", make, re.M).group(1).strip()) / "tests" / "data" / "basetest.fil"
+    """basetest.fil under the reference checkout the checkers are built from
+    (GAFFA_REFERENCE_DIR, as __graft_entry__.build uses it)."""
+    import __graft_entry__
+    return Path(__graft_entry__.REFERENCE_DIR) / "tests" / "data" / "basetest.fil"
 
 
 REFERENCE_FIL = _reference_fil()
