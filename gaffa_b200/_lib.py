@@ -158,6 +158,8 @@ _SIGNATURES = [
     ("gf_last_error", C.c_char_p, []),
     ("gf_status_string", C.c_char_p, [C.c_int]),
     ("gf_build_info", C.c_char_p, []),
+    ("gf_cuda_device_count", C.c_int, [C.POINTER(i32)]),
+    ("gf_cuda_runtime_version", C.c_int, [C.POINTER(i32)]),
     ("gf_make_riptide_ffa_plan", C.c_int, [u64, dbl, C.POINTER(PlanOptions), vp, u64, C.POINTER(u64), vp,
                                            u64, C.POINTER(u64)]),
     ("gf_downsampled_size", C.c_int, [u64, dbl, C.POINTER(u64)]),

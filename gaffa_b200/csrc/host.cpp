@@ -245,6 +245,32 @@ extern "C" const char* gf_build_info(void) {
          "fold_reduce_kernel, synth_kernel";
 }
 
+// cuda_device_count / cuda_runtime_version (src/gaffa/vector_add.cu:75-86):
+// the devices visible to the runtime this library links, and its version
+extern "C" int gf_cuda_device_count(int32_t* count) {
+  return guarded([&] {
+    check_arg(count != nullptr, "null argument");
+    int n = 0;
+    const cudaError_t e = cudaGetDeviceCount(&n);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) {
+      cudaGetLastError();  // clear the sticky-free error and report no devices
+      n = 0;
+    } else {
+      cuda_check(e, "cudaGetDeviceCount");
+    }
+    *count = n;
+  });
+}
+
+extern "C" int gf_cuda_runtime_version(int32_t* version) {
+  return guarded([&] {
+    check_arg(version != nullptr, "null argument");
+    int v = 0;
+    cuda_check(cudaRuntimeGetVersion(&v), "cudaRuntimeGetVersion");
+    *version = v;
+  });
+}
+
 extern "C" int gf_make_riptide_ffa_plan(uint64_t nsamples, double tsamp, const gf_plan_options* options,
                                         gf_ffa_task* tasks, uint64_t task_capacity, uint64_t* ntasks,
                                         uint64_t* widths, uint64_t width_capacity, uint64_t* nwidths) {

@@ -44,6 +44,12 @@ const char* gf_last_error(void);
 const char* gf_status_string(int status);
 /* Library build description (architecture, kernel list) for diagnostics. */
 const char* gf_build_info(void);
+/* Replace cuda_device_count / cuda_runtime_version (src/gaffa/vector_add.cu:75-86,
+ * bound as gaffa._core.cuda_device_count / cuda_runtime_version): visible
+ * devices (0 when there is no device or driver) and the CUDA runtime version
+ * of this library (e.g. 12090). */
+int gf_cuda_device_count(int32_t* count);
+int gf_cuda_runtime_version(int32_t* version);
 
 /* ------------------------------------------------------------------------ */
 /* FFA plan (host)                                                           */
