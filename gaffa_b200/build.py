@@ -17,6 +17,10 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libgaffa_b200.so"
 SOURCES = ["host.cpp", "dedisperse.cu", "preprocess.cu", "ffa.cu", "fold.cu", "synth.cu", "filterbank.cu", "proposal.cu"]
+# gaffa's C++ API (include/gaffa/*.h) over the C ABI: plain C++20 host code
+CXX_SOURCES = ["cxx_api.cpp"]
+CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra", f"-I{ROOT / 'include'}",
+             "-I/usr/local/cuda/include"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",
@@ -35,16 +39,19 @@ def _nvcc() -> str:
 
 
 def _compile(src: Path, obj: Path) -> None:
-    cmd = [_nvcc(), *NVCC_FLAGS, "-x", "cu", "-c", str(src), "-o", str(obj)]
+    if src.name in CXX_SOURCES:
+        cmd = [shutil.which("g++") or "g++", *CXX_FLAGS, "-c", str(src), "-o", str(obj)]
+    else:
+        cmd = [_nvcc(), *NVCC_FLAGS, "-x", "cu", "-c", str(src), "-o", str(obj)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stderr}")
+        raise RuntimeError(f"compile failed for {src.name}:\n{r.stderr}")
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
-    srcs = [CSRC / s for s in SOURCES]
-    headers = list(CSRC.glob("*.cuh")) + [ROOT / "include" / "gaffa_b200.h"]
+    srcs = [CSRC / s for s in SOURCES + CXX_SOURCES]
+    headers = list(CSRC.glob("*.cuh")) + [ROOT / "include" / "gaffa_b200.h"] + list((ROOT / "include" / "gaffa").glob("*.h"))
     newest_header = max(h.stat().st_mtime for h in headers)
     jobs = []
     objs = []
