@@ -153,6 +153,10 @@ NO_HARMONIC_PARENT = (1 << 64) - 1
 assert C.sizeof(FfaTask) == TASK_DTYPE.itemsize == 72
 assert PEAK_RECORD_DTYPE.itemsize == 24 and PEAK_DTYPE.itemsize == 96
 
+class PeakSegment(C.Structure):
+    _fields_ = [("record_begin", u64), ("record_count", u64), ("series_offset", u64)]
+
+
 # (name, restype, argtypes) for every entry point of include/gaffa_b200.h
 _SIGNATURES = [
     ("gf_last_error", C.c_char_p, []),
@@ -193,6 +197,9 @@ _SIGNATURES = [
     ("gf_ffa_batch_expand_peaks", C.c_int, [vp, vp, u64, vp, vp, vp, vp, vp]),
     ("gf_sort_peaks", C.c_int, [vp, u64]),
     ("gf_select_candidates", C.c_int, [vp, u64, dbl, C.POINTER(CandidateOptions), vp, u64, C.POINTER(u64)]),
+    ("gf_select_candidates_device_workspace", C.c_int, [u64, C.POINTER(u64)]),
+    ("gf_select_candidates_device", C.c_int, [vp, vp, C.POINTER(PeakSegment), u64, dbl, dbl, dbl,
+                                              C.POINTER(CandidateOptions), vp, u64, vp, u64, C.POINTER(u64), vp]),
     ("gf_fold_workspace_bytes", u64, [u64, u64]),
     ("gf_fold_time_series", C.c_int, [vp, i32, u64, dbl, dbl, u64, u64, vp, vp, vp, vp]),
     ("gf_synth_generate", C.c_int, [C.POINTER(SynthDesc), u64, u64, vp, vp]),

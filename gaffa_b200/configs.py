@@ -36,6 +36,7 @@ class SearchConfig:
     ndm_per_nominal: int = 32
     frequency_cluster_radius: float = 0.1
     dm_cluster_radius: int = 1
+    device_candidates: bool = False        # select candidates on the device (10^7+ raw peaks)
 
     @property
     def dms(self) -> np.ndarray:
@@ -112,7 +113,8 @@ def wide_subband(seed: int = 0, nsamples: int = 1 << 22, nchans: int = 4096,
     return SearchConfig(
         name="wide_subband", obs=obs, dm_low=0.0, dm_step=dm_step, ndm=ndm,
         period_min=0.1, period_max=10.0, duty_cycle_max=0.1, dedispersion="subband",
-        subband_channels=nchans // 64, ndm_per_nominal=int(math.ceil(20.0 / dm_step)))
+        subband_channels=nchans // 64, ndm_per_nominal=int(math.ceil(20.0 / dm_step)),
+        device_candidates=True)
 
 
 def batched_uneven(seed: int = 0, nobs: int = 64, nchans_choices=(1024, 2048, 4096), log2_nsamples=(20.0, 23.0),

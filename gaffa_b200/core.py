@@ -362,6 +362,25 @@ class FfaProgram:
     def kernel_launches(self) -> int:
         return int(self.info.nclasses)
 
+    def count(self, prepared: torch.Tensor, nseries: int, snr_threshold: float, max_peaks: int = 0,
+              stream=None) -> int:
+        """Peak records of the last search_async, left on the device in
+        self.peaks (the first count * 24 bytes); grows the buffer and re-runs
+        on overflow as collect does."""
+        while True:
+            counts = self.counters.cpu()
+            if int(counts[1]) & _lib.STATUS_SCHEDULE:
+                raise RuntimeError("FFA block schedule exceeded its shared-memory tile")
+            n = int(counts[0])
+            if n <= self.capacity:
+                break
+            self.capacity = int(n * 1.25) + 1024
+            self.peaks = torch.empty(self.capacity * 24, dtype=torch.uint8, device=self.device)
+            self.search_async(prepared, nseries, snr_threshold, stream)
+        if max_peaks and n > max_peaks * nseries:
+            raise RuntimeError("FFA detection peak count exceeded max_peaks safety guard")
+        return n
+
     def collect(self, prepared: torch.Tensor, nseries: int, snr_threshold: float, max_peaks: int = 0,
                 stream=None) -> np.ndarray:
         """Reads the records of the last search_async; on a peak-buffer
@@ -555,6 +574,43 @@ def select_candidates(peaks: np.ndarray, observation_seconds: float, frequency_c
     check(_lib.lib().gf_select_candidates(ptr(peaks), len(peaks), observation_seconds, C.byref(o), ptr(out),
                                           len(out), C.byref(n)))
     return out
+
+
+def select_candidates_device(program: "FfaProgram", records: torch.Tensor, segments, dm_low: float, dm_step: float,
+                             observation_seconds: float, frequency_cluster_radius: float = 0.1,
+                             dm_cluster_radius: int = 1, cluster_across_widths: bool = True,
+                             max_candidates: int = 0, stream=None) -> np.ndarray:
+    """select_candidates_cpu (src/gaffa/candidate.cpp:175-212) over compact
+    device peak records (uint8 tensor of 24-byte records) without expanding
+    them on the host: segments are (record_begin, record_count, dm_offset)
+    runs of records of one FfaProgram search each.  Equals select_candidates
+    of the expanded, sorted peaks."""
+    segs = list(segments)
+    arr = (_lib.PeakSegment * max(1, len(segs)))()
+    total = 0
+    for i, (b, n, off) in enumerate(segs):
+        arr[i] = _lib.PeakSegment(int(b), int(n), int(off))
+        total += int(n)
+    o = _lib.CandidateOptions(frequency_cluster_radius, dm_cluster_radius, int(cluster_across_widths), 0,
+                              max_candidates)
+    if total == 0:
+        return np.zeros(0, _lib.CAND_DTYPE)
+    ws_bytes = _lib.u64()
+    with torch.cuda.device(program.device):
+        check(_lib.lib().gf_select_candidates_device_workspace(total, C.byref(ws_bytes)))
+        ws = torch.empty(int(ws_bytes.value), dtype=torch.uint8, device=program.device)
+        n = _lib.u64()
+        # usually far fewer candidates than peaks: a bounded first guess, and a
+        # second call only when the candidates exceed it
+        out = np.zeros(min(total, 1 << 16), _lib.CAND_DTYPE)
+        for _ in range(2):
+            check(_lib.lib().gf_select_candidates_device(program._h, ptr(records), arr, len(segs), dm_low, dm_step,
+                                                         observation_seconds, C.byref(o), ptr(ws), ws.numel(),
+                                                         ptr(out), len(out), C.byref(n), _stream(stream)))
+            if n.value <= len(out):
+                break
+            out = np.zeros(n.value, _lib.CAND_DTYPE)
+    return out[: n.value]
 
 
 def dedisperse_spectrum(filterbank: torch.Tensor, frequency_mhz, dm: float, tsamp: float,

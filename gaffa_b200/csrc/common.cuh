@@ -10,6 +10,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "gaffa_b200.h"
 
@@ -129,5 +130,14 @@ struct DeviceBlob {
 // round-half-away-from-zero of 4148.808 * dm * (f^-2 - fref^-2) / tsamp, in
 // FP64 with the reference's operation order.
 int32_t delay_bins(double dm, double f, double fref, double tsamp);
+
+// One plan task's period arithmetic inputs (for device peak expansion).
+struct PeakTaskInfo {
+  double effective_tsamp;
+  uint64_t bins, rows;
+};
+// The task table, width trials and device of a single-plan FFA program.
+void ffa_program_peak_tables(const gf_ffa_program* program, std::vector<PeakTaskInfo>& tasks,
+                             std::vector<uint64_t>& widths, int& device);
 
 }  // namespace gf

@@ -1313,6 +1313,18 @@ void expand_record(const gf_ffa_program* P, const gf_peak_record& r, uint64_t se
 
 }  // namespace
 
+namespace gf {
+void ffa_program_peak_tables(const gf_ffa_program* P, std::vector<PeakTaskInfo>& tasks, std::vector<uint64_t>& widths,
+                             int& device) {
+  check_arg(P != nullptr, "null argument");
+  check_arg(!P->batched && P->members.size() == 1, "device candidate selection takes a single-plan FFA program");
+  tasks.clear();
+  for (const gf_ffa_task& t : P->tasks) tasks.push_back(PeakTaskInfo{t.effective_tsamp, t.bins, t.rows});
+  widths = P->members[0].widths;
+  device = P->device;
+}
+}  // namespace gf
+
 extern "C" int gf_ffa_program_create(const gf_ffa_task* tasks, uint64_t ntasks, const uint64_t* widths,
                                      uint64_t nwidths, uint64_t max_series, int32_t device_id,
                                      gf_ffa_program** out) {

@@ -218,6 +218,12 @@ bool better_candidate(const gf_candidate& l, const gf_candidate& r) {
 }
 
 }  // namespace
+
+// candidate.cpp:205-206: rank by is_better_candidate
+void rank_candidates(std::vector<gf_candidate>& candidates) {
+  std::sort(candidates.begin(), candidates.end(), better_candidate);
+}
+
 }  // namespace gf
 
 using namespace gf;

@@ -35,6 +35,9 @@ class SearchResult:
     ranked: np.ndarray | None = None
     harmonics: np.ndarray | None = None
     unique_candidates: np.ndarray | None = None
+    # raw peaks found; equals len(peaks) unless candidates were selected on the
+    # device, where the raw peaks stay on the device and `peaks` is empty
+    peak_count: int = 0
 
     @property
     def dm_trial_samples(self) -> int:
@@ -70,7 +73,14 @@ class DmSearch:
                  algorithm: str = "brute", subband_channels: int = 32, ndm_per_nominal: int = 32,
                  frequency_cluster_radius: float = 0.1, dm_cluster_radius: int = 1, fold_nbin: int = 64,
                  dm_batch: int | None = None, memory_budget: int | None = None, device_id: int = 0,
-                 harmonic_options=None, launch_shape: tuple[int, int] | None = None):
+                 harmonic_options=None, launch_shape: tuple[int, int] | None = None,
+                 device_candidates: bool = False, peak_capacity: int | None = None):
+        """device_candidates: keep the raw peak records on the device and select
+        candidates there (gf_select_candidates_device) -- for workloads with
+        10^7 or more raw peaks, whose host expansion and sort would dominate;
+        the result's `peaks` is then empty and `peak_count` counts them.
+        peak_capacity: initial peak-record capacity per DM batch (it grows and
+        the batch is re-searched when exceeded)."""
         self.device = torch.device("cuda", device_id)
         freq = np.asarray(frequency_mhz, dtype=np.float64)
         self.frequency_low_mhz, self.frequency_high_mhz = float(freq.min()), float(freq.max())
@@ -104,6 +114,10 @@ class DmSearch:
                                           normalise=True, reject_constant=True, max_series=self.dm_batch,
                                           device_id=device_id)
         self.ffa = core.FfaProgram(plan, max_series=self.dm_batch, device_id=device_id)
+        self.device_candidates = device_candidates
+        if peak_capacity is not None and peak_capacity > self.ffa.capacity:
+            self.ffa.capacity = int(peak_capacity)
+            self.ffa.peaks = torch.empty(self.ffa.capacity * 24, dtype=torch.uint8, device=self.device)
         self._series = torch.empty(self.dm_batch * self.out_stride, dtype=torch.int32, device=self.device)
         self._prepared = torch.empty((self.dm_batch, self.ffa.prepared_floats), dtype=torch.float32,
                                      device=self.device)
@@ -147,12 +161,31 @@ class DmSearch:
                 self.ffa.prepare(dd.view(torch.float32), cnt, stats, out=self._prepared)
             with _StageTimer(timers, "ffa"):
                 self.ffa.search_async(self._prepared, cnt, self.snr_threshold)
-            rec = self.ffa.collect(self._prepared, cnt, self.snr_threshold)
-            parts.append(self.ffa.expand(rec, b0, self.dm_low, self.dm_step))
+            if self.device_candidates:
+                n = self.ffa.count(self._prepared, cnt, self.snr_threshold)
+                parts.append((self.ffa.peaks[: n * 24].clone(), n, b0))
+            else:
+                rec = self.ffa.collect(self._prepared, cnt, self.snr_threshold)
+                parts.append(self.ffa.expand(rec, b0, self.dm_low, self.dm_step))
             launches += dd_kernels + 4 + 1 + ffa_kernels
         self.pre.synchronize()
+        if self.device_candidates:
+            return parts, launches
         peaks = np.concatenate(parts) if parts else np.zeros(0, _lib.PEAK_DTYPE)
         return peaks, launches
+
+    def _device_candidates(self, parts, tobs: float) -> tuple[np.ndarray, int]:
+        """Candidates of the device-resident records of every batch."""
+        segments, at = [], 0
+        for _, n, b0 in parts:
+            segments.append((at, n, b0))
+            at += n
+        if at == 0:
+            return np.zeros(0, _lib.CAND_DTYPE), 0
+        records = torch.cat([r for r, _, _ in parts]) if len(parts) > 1 else parts[0][0]
+        cands = core.select_candidates_device(self.ffa, records, segments, self.dm_low, self.dm_step, tobs,
+                                              self.frequency_cluster_radius, self.dm_cluster_radius)
+        return cands, at
 
     def fold_candidate(self, staged: torch.Tensor, dm_index: int, period: float):
         """fold_time_series of the candidate's uint32 dedispersed series."""
@@ -233,9 +266,15 @@ class DmSearch:
         t1 = time.perf_counter()
         peaks, launches = self.search_staged(staged, timers, dm_ranges)
         t2 = time.perf_counter()
-        peaks = core.sort_peaks(peaks)
         tobs = self.nsamples * self.tsamp if observation_seconds is None else observation_seconds
-        cands = core.select_candidates(peaks, tobs, self.frequency_cluster_radius, self.dm_cluster_radius)
+        if self.device_candidates:
+            launches += len(peaks) + 9      # expansion per batch, keys, splits, gather (plus the sorts and scans)
+            cands, npeaks = self._device_candidates(peaks, tobs)
+            peaks = np.zeros(0, _lib.PEAK_DTYPE)
+        else:
+            peaks = core.sort_peaks(peaks)
+            npeaks = len(peaks)
+            cands = core.select_candidates(peaks, tobs, self.frequency_cluster_radius, self.dm_cluster_radius)
         # the step after candidate selection in the reference's drivers
         # (cuda_dm_search_benchmark.cpp:287-292)
         ranked, rel = core.flag_harmonics(cands, tobs, self.frequency_low_mhz, self.frequency_high_mhz,
@@ -250,7 +289,7 @@ class DmSearch:
         t.update(stage=t1 - t0, search=t2 - t1, candidates=t3 - t2, fold=t4 - t3, total=t4 - t0)
         return SearchResult(peaks=peaks, candidates=cands, fold_profile=prof, fold_exposure=expo, nout=self.nout,
                             ndm=self.ndm, timings=t, gpu_launches=launches + 1, ranked=ranked, harmonics=rel,
-                            unique_candidates=unique)
+                            unique_candidates=unique, peak_count=npeaks)
 
 
 def from_config(cfg, **overrides) -> DmSearch:
@@ -263,6 +302,6 @@ def from_config(cfg, **overrides) -> DmSearch:
               snr_threshold=cfg.snr_threshold, nbits=obs.nbits, algorithm=cfg.dedispersion,
               subband_channels=cfg.subband_channels, ndm_per_nominal=cfg.ndm_per_nominal,
               frequency_cluster_radius=cfg.frequency_cluster_radius, dm_cluster_radius=cfg.dm_cluster_radius,
-              fold_nbin=cfg.fold_nbin)
+              fold_nbin=cfg.fold_nbin, device_candidates=cfg.device_candidates)
     kw.update(overrides)
     return DmSearch(**kw)

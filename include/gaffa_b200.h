@@ -474,6 +474,38 @@ int gf_select_candidates(const gf_peak* peaks, uint64_t npeaks,
                          gf_candidate* out, uint64_t capacity,
                          uint64_t* ncandidates);
 
+/* A run of compact device peak records from one gf_ffa_search call:
+ * records [record_begin, record_begin + record_count) of the record array,
+ * whose series s is DM trial series_offset + s. */
+typedef struct {
+  uint64_t record_begin;
+  uint64_t record_count;
+  uint64_t series_offset;
+} gf_peak_segment;
+
+/* select_candidates_cpu (src/gaffa/candidate.cpp:175-212) over compact
+ * device records, for peak sets too large to expand and sort on the host:
+ * the records are expanded on the device (make_ffa_peak,
+ * ffa_detection.cpp:266-284; dm = dm_low + index * dm_step), ordered by
+ * stable device radix sorts into the reference's peak and group orders,
+ * split and reduced per cluster on the device; the candidates (best peak,
+ * count, DM and frequency extent) are ranked on the host
+ * (is_better_candidate, candidate.cpp:48-62) and written to out (two-call
+ * pattern on capacity; synchronises the stream).  The result equals
+ * gf_select_candidates on the expanded records.  program is the
+ * single-plan FFA program that produced the records; dev_workspace needs
+ * gf_select_candidates_device_workspace(total records) bytes. */
+int gf_select_candidates_device_workspace(uint64_t npeaks, uint64_t* bytes);
+int gf_select_candidates_device(const gf_ffa_program* program,
+                                const gf_peak_record* dev_records,
+                                const gf_peak_segment* segments, uint64_t nsegments,
+                                double dm_low, double dm_step,
+                                double observation_seconds,
+                                const gf_candidate_options* options,
+                                void* dev_workspace, uint64_t workspace_bytes,
+                                gf_candidate* out, uint64_t capacity,
+                                uint64_t* ncandidates, void* stream);
+
 /* HarmonicContext, include/gaffa/harmonic.h:16-20. */
 typedef struct {
   double observation_seconds;
