@@ -61,6 +61,8 @@ def parse_args():
                     help="fraction of DM windows searched (default: the shipped model's)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven-workload measurement")
     ap.add_argument("--batched-observations", type=int, default=12)
+    ap.add_argument("--no-wide-subband", action="store_true",
+                    help="skip the wide-range subband measurement at its configured size")
     return ap.parse_args()
 
 
@@ -156,7 +158,13 @@ def algorithmic_bytes(stage: str, cfg, ds, units: int) -> float:
     if stage == "dedisperse":
         # input read once + uint32 output written
         in_bytes = obs.nsamples * obs.nchans * (1 if obs.nbits == 8 else 0.25)
-        return units * (4.0 + in_bytes / (cfg.ndm * ds.nout))
+        per_unit = 4.0 + in_bytes / (cfg.ndm * ds.nout)
+        if cfg.dedispersion == "subband":
+            # plus the uint8 stage-1 intermediate, written once and read once
+            n_nom = -(-cfg.ndm // cfg.ndm_per_nominal)
+            inter = float(n_nom) * (obs.nchans // cfg.subband_channels) * obs.nsamples
+            per_unit += 2.0 * inter / (cfg.ndm * ds.nout)
+        return units * per_unit
     if stage == "preprocess":
         return units * 8.0                    # uint32 in, float out, in place
     if stage == "prepare":
@@ -410,6 +418,54 @@ def batched_measurement(nobs: int, device_id: int, case: str = "reduced") -> dic
             "tuned_dedispersion_shapes": tuner.cache, "case": case, "laws": BATCHED_CASES[case]}
 
 
+def wide_subband_measurement(device_id: int) -> dict:
+    """The wide-range subband workload at its configured size (2-bit, 4096
+    channels over 300-400 MHz, 2^22 samples, 64 subbands, nominal DMs every
+    20, 8192 DM trials over 0-3000, 16 pulsars, 50 Hz narrowband and 0.1 Hz
+    impulse RFI): one warm-up and one timed search from an HBM-resident
+    packed filterbank, with candidate selection on the device (its ~10^8 raw
+    peaks never leave the GPU).  Reports DM-trial*samples/s, the stage times,
+    the subband dedispersion's byte-add rate and algorithmic bytes, and the
+    raw-peak and candidate counts."""
+    import torch
+    from gaffa_b200 import configs, core, search
+    cfg = configs.wide_subband()
+    obs = cfg.obs
+    raw = core.synth_generate(obs, device_id=device_id)
+    ds = search.from_config(cfg, device_id=device_id, peak_capacity=None)
+    ds.run(raw)                                      # warm-up; sizes the peak buffer
+    timers = {}
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    res = ds.run(raw, timers=timers)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    stage = {k: round(sum(x.elapsed_time(y) for x, y in v), 2) for k, v in timers.items()}
+    units = cfg.ndm * ds.nout
+    n_nom = -(-cfg.ndm // cfg.ndm_per_nominal)
+    n_sb = obs.nchans // cfg.subband_channels
+    stage1_adds = float(n_nom) * obs.nchans * obs.nsamples
+    stage2_adds = float(cfg.ndm) * n_sb * ds.nout
+    # packed input read, uint8 intermediate written and read, uint32 output written
+    inter = float(n_nom) * n_sb * obs.nsamples
+    alg = obs.nchans * obs.nsamples / 4 + 2 * inter + 4.0 * units
+    dd_s = stage.get("dedisperse", 0.0) / 1e3
+    out = {"value": units / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "nout": ds.nout, "ndm": cfg.ndm,
+           "dm_batch": ds.dm_batch, "stage_ms": stage, "raw_peaks": res.peak_count,
+           "candidates": len(res.candidates), "candidate_selection": "device",
+           "dedisperse": {"stage1_adds": stage1_adds, "stage2_adds": stage2_adds,
+                          "adds_per_s": (stage1_adds + stage2_adds) / dd_s if dd_s else None,
+                          "algorithmic_bytes": alg, "achieved_gbs": alg / dd_s / 1e9 if dd_s else None},
+           "config": {"workload": cfg.name, "nchans": obs.nchans, "nsamples": obs.nsamples, "nbits": obs.nbits,
+                      "subbands": n_sb, "ndm_per_nominal": cfg.ndm_per_nominal}}
+    del ds, raw
+    torch.cuda.empty_cache()
+    return out
+
+
 def cpu_baseline(cfg, host_input, min_dms: int) -> dict:
     """The reference CPU path on a contiguous sample of at least `min_dms` DM
     trials of the same observation (ReferenceCpuPath), timed once."""
@@ -442,10 +498,12 @@ def main():
     from gaffa_b200 import core, search
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    batched = batched_small = None
+    batched = batched_small = wide = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_measurement(args.batched_observations, local, "reduced")
         batched_small = batched_measurement(64, local, "small")
+    if rank == 0 and world == 1 and not args.no_wide_subband and args.workload != "wide_subband":
+        wide = wide_subband_measurement(local)
     cfg = workload(args, rank)
     obs = cfg.obs
     raw = core.synth_generate(obs, device_id=local)          # device-resident filterbank
@@ -576,6 +634,7 @@ def main():
             "proposal": prop,
             "batched": batched,
             "batched_small": batched_small,
+            "wide_subband": wide,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

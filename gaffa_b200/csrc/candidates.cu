@@ -53,8 +53,13 @@ struct DevPeak {
 };
 static_assert(sizeof(DevPeak) == 40, "DevPeak is 40 bytes");
 
+// Per-cluster aggregate.  The best peak is carried as its rank in the
+// is_better_dm_peak order (0 = best), so merging two aggregates is pure
+// arithmetic: the reduction never reads memory through a carried value
+// (a device reduction may apply its operator to the unloaded tail items of
+// its last tile, whose fields are arbitrary).
 struct ClusterAgg {
-  uint32_t best;  // index (into the expanded peaks) of the cluster's best peak
+  uint32_t best_rank;
   uint32_t count;
   uint32_t dm_min, dm_max;
   double f_min, f_max;
@@ -68,18 +73,6 @@ __device__ __forceinline__ uint32_t snr_desc_key(float f) {
   return ~asc;
 }
 
-// is_better_dm_peak (dm_search.cpp:89-100 over ffa_peak.cpp:16-45) for
-// finite peaks; dm is monotone in dm_index
-__device__ __forceinline__ bool better(const DevPeak& l, const DevPeak& r) {
-  if (l.snr != r.snr) return l.snr > r.snr;
-  if (l.period != r.period) return l.period < r.period;
-  if (l.frequency != r.frequency) return l.frequency < r.frequency;
-  if (l.width != r.width) return l.width < r.width;
-  if (l.phase != r.phase) return l.phase < r.phase;
-  if (l.shift != r.shift) return l.shift < r.shift;
-  if (l.bins != r.bins) return l.bins < r.bins;
-  return l.dm_index < r.dm_index;
-}
 
 // make_ffa_peak with trial_period (ffa_detection.cpp:115-124,266-284), in the
 // operation order of the host expansion.  status bit 1: a non-finite value
@@ -153,6 +146,42 @@ __global__ void peak_order_key_kernel(const DevPeak* __restrict__ peaks, const u
   keys[i] = k;
 }
 
+// keys of the least-significant-first passes of is_better_dm_peak
+// (dm_search.cpp:89-100 over ffa_peak.cpp:16-45; finite peaks, dm follows
+// dm_index, equal periods give equal frequencies):
+//   0: DM index   1: phase, shift, bins   2: width   3: period   4: S/N descending
+__global__ void better_key_kernel(const DevPeak* __restrict__ peaks, const uint32_t* __restrict__ idx, uint64_t n,
+                                  int pass, uint64_t* __restrict__ keys) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+  if (i >= n) return;
+  const DevPeak p = peaks[idx[i]];
+  uint64_t k;
+  switch (pass) {
+    case 0:
+      k = p.dm_index;
+      break;
+    case 1:
+      k = (static_cast<uint64_t>(p.phase) << 48) | (static_cast<uint64_t>(p.shift) << 16) | p.bins;
+      break;
+    case 2:
+      k = p.width;
+      break;
+    case 3:
+      k = static_cast<uint64_t>(__double_as_longlong(p.period));
+      break;
+    default:
+      k = snr_desc_key(p.snr);
+      break;
+  }
+  keys[i] = k;
+}
+
+// rank[order[r]] = r
+__global__ void rank_kernel(const uint32_t* __restrict__ order, uint64_t n, uint32_t* __restrict__ rank) {
+  const uint64_t r = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
+  if (r < n) rank[order[r]] = static_cast<uint32_t>(r);
+}
+
 // 1 where the sorted frequency steps by more than the radius (candidate.cpp:190-199)
 __global__ void frequency_split_kernel(const DevPeak* __restrict__ peaks, const uint32_t* __restrict__ idx,
                                        uint64_t n, double radius_hz, uint32_t* __restrict__ flag) {
@@ -177,9 +206,9 @@ __global__ void group_key_kernel(const DevPeak* __restrict__ peaks, const uint32
 // cluster starts (append_dm_clusters, candidate.cpp:140-171) and the
 // per-peak aggregate seeds
 __global__ void cluster_split_kernel(const DevPeak* __restrict__ peaks, const uint32_t* __restrict__ idx,
-                                     const uint64_t* __restrict__ keys, uint64_t n, int across_widths,
-                                     uint64_t dm_radius, uint32_t* __restrict__ flag,
-                                     ClusterAgg* __restrict__ seed) {
+                                     const uint32_t* __restrict__ rank, const uint64_t* __restrict__ keys,
+                                     uint64_t n, int across_widths, uint64_t dm_radius,
+                                     uint32_t* __restrict__ flag, ClusterAgg* __restrict__ seed) {
   const uint64_t i = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
   if (i >= n) return;
   const DevPeak p = peaks[idx[i]];
@@ -192,14 +221,13 @@ __global__ void cluster_split_kernel(const DevPeak* __restrict__ peaks, const ui
     f = (new_group || !same_width || !same_dm) ? 1u : 0u;
   }
   flag[i] = f;
-  seed[i] = ClusterAgg{idx[i], 1u, p.dm_index, p.dm_index, p.frequency, p.frequency};
+  seed[i] = ClusterAgg{rank[idx[i]], 1u, p.dm_index, p.dm_index, p.frequency, p.frequency};
 }
 
 struct MergeClusters {
-  const DevPeak* peaks;
   __device__ __forceinline__ ClusterAgg operator()(const ClusterAgg& a, const ClusterAgg& b) const {
     ClusterAgg c;
-    c.best = better(peaks[b.best], peaks[a.best]) ? b.best : a.best;
+    c.best_rank = min(a.best_rank, b.best_rank);
     c.count = a.count + b.count;
     c.dm_min = min(a.dm_min, b.dm_min);
     c.dm_max = max(a.dm_max, b.dm_max);
@@ -209,16 +237,18 @@ struct MergeClusters {
   }
 };
 
-__global__ void gather_best_kernel(const DevPeak* __restrict__ peaks, const ClusterAgg* __restrict__ agg,
-                                   const uint32_t* __restrict__ nclusters, DevPeak* __restrict__ best) {
+__global__ void gather_best_kernel(const DevPeak* __restrict__ peaks, const uint32_t* __restrict__ order,
+                                   const ClusterAgg* __restrict__ agg, const uint32_t* __restrict__ nclusters,
+                                   uint64_t n, DevPeak* __restrict__ best) {
   const uint64_t i = static_cast<uint64_t>(blockIdx.x) * kThreads + threadIdx.x;
-  if (i < *nclusters) best[i] = peaks[agg[i].best];
+  if (i < *nclusters && agg[i].best_rank < n) best[i] = peaks[order[agg[i].best_rank]];
 }
 
 unsigned blocks_for(uint64_t n) { return static_cast<unsigned>(std::max<uint64_t>(1, ceil_div(n, kThreads))); }
 
 struct Layout {
-  size_t peaks, keys_a, keys_b, idx_a, idx_b, u32_a, u32_b, seeds, aggs, best, counters, temp, temp_bytes, total;
+  size_t peaks, keys_a, keys_b, idx_a, idx_b, order_a, order_b, rank, u32_a, u32_b, seeds, aggs, best, counters,
+      temp, temp_bytes, total;
 };
 
 // workspace carve-up for n peaks (256-byte aligned pieces)
@@ -236,7 +266,7 @@ Layout layout_for(uint64_t n, cudaStream_t s) {
   cuda_check(cub::DeviceReduce::ReduceByKey(nullptr, t, static_cast<uint32_t*>(nullptr),
                                             static_cast<uint32_t*>(nullptr), static_cast<ClusterAgg*>(nullptr),
                                             static_cast<ClusterAgg*>(nullptr), static_cast<uint32_t*>(nullptr),
-                                            MergeClusters{nullptr}, static_cast<int64_t>(n), s),
+                                            MergeClusters{}, static_cast<int64_t>(n), s),
              "cub::DeviceReduce size");
   temp = std::max(temp, t);
   Layout L{};
@@ -251,6 +281,9 @@ Layout layout_for(uint64_t n, cudaStream_t s) {
   L.keys_b = take(n * 8);
   L.idx_a = take(n * 4);
   L.idx_b = take(n * 4);
+  L.order_a = take(n * 4);
+  L.order_b = take(n * 4);
+  L.rank = take(n * 4);
   L.u32_a = take(n * 4);
   L.u32_b = take(n * 4);
   L.seeds = take(n * sizeof(ClusterAgg));
@@ -312,6 +345,9 @@ extern "C" int gf_select_candidates_device(const gf_ffa_program* program, const 
     uint64_t* kb = reinterpret_cast<uint64_t*>(ws + L.keys_b);
     uint32_t* ia = reinterpret_cast<uint32_t*>(ws + L.idx_a);
     uint32_t* ib = reinterpret_cast<uint32_t*>(ws + L.idx_b);
+    uint32_t* oa = reinterpret_cast<uint32_t*>(ws + L.order_a);
+    uint32_t* ob = reinterpret_cast<uint32_t*>(ws + L.order_b);
+    uint32_t* rank = reinterpret_cast<uint32_t*>(ws + L.rank);
     uint32_t* ua = reinterpret_cast<uint32_t*>(ws + L.u32_a);
     uint32_t* ub = reinterpret_cast<uint32_t*>(ws + L.u32_b);
     ClusterAgg* seeds = reinterpret_cast<ClusterAgg*>(ws + L.seeds);
@@ -341,9 +377,17 @@ extern "C" int gf_select_candidates_device(const gf_ffa_program* program, const 
     cuda_check(cudaGetLastError(), "expand_kernel launch");
     const int64_t nn = static_cast<int64_t>(n);
     size_t temp_bytes = L.temp_bytes;
+    cub::DoubleBuffer<uint64_t> keys(ka, kb);
+    // rank of every peak in the is_better_dm_peak order: five stable passes
+    iota_kernel<<<blocks_for(n), kThreads, 0, s>>>(oa, n);
+    cub::DoubleBuffer<uint32_t> order(oa, ob);
+    for (int pass = 0; pass < 5; ++pass) {
+      better_key_kernel<<<blocks_for(n), kThreads, 0, s>>>(peaks, order.Current(), n, pass, keys.Current());
+      cuda_check(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, order, nn, 0, 64, s), "best-peak sort");
+    }
+    rank_kernel<<<blocks_for(n), kThreads, 0, s>>>(order.Current(), n, rank);
     // peak_order: four stable passes, least significant key first
     iota_kernel<<<blocks_for(n), kThreads, 0, s>>>(ia, n);
-    cub::DoubleBuffer<uint64_t> keys(ka, kb);
     cub::DoubleBuffer<uint32_t> idx(ia, ib);
     for (int pass = 0; pass < 4; ++pass) {
       peak_order_key_kernel<<<blocks_for(n), kThreads, 0, s>>>(peaks, idx.Current(), n, pass, keys.Current());
@@ -358,14 +402,14 @@ extern "C" int gf_select_candidates_device(const gf_ffa_program* program, const 
                                                          keys.Current());
     cuda_check(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, idx, nn, 0, 64, s), "group sort");
     // clusters and their aggregates
-    cluster_split_kernel<<<blocks_for(n), kThreads, 0, s>>>(peaks, idx.Current(), keys.Current(), n,
+    cluster_split_kernel<<<blocks_for(n), kThreads, 0, s>>>(peaks, idx.Current(), rank, keys.Current(), n,
                                                              o->cluster_across_widths, o->dm_cluster_radius, ua,
                                                              seeds);
     cuda_check(cub::DeviceScan::InclusiveSum(temp, temp_bytes, ua, ub, nn, s), "cluster scan");
     cuda_check(cub::DeviceReduce::ReduceByKey(temp, temp_bytes, ub, ua, seeds, aggs, counters + 1,
-                                              MergeClusters{peaks}, nn, s),
+                                              MergeClusters{}, nn, s),
                "cluster reduce");
-    gather_best_kernel<<<blocks_for(n), kThreads, 0, s>>>(peaks, aggs, counters + 1, best);
+    gather_best_kernel<<<blocks_for(n), kThreads, 0, s>>>(peaks, order.Current(), aggs, counters + 1, n, best);
     cuda_check(cudaGetLastError(), "candidate kernels");
     uint32_t host_counters[2] = {0, 0};
     cuda_check(cudaMemcpyAsync(host_counters, counters, 8, cudaMemcpyDeviceToHost, s), "candidate counters");
