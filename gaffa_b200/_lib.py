@@ -220,6 +220,8 @@ _SIGNATURES = [
     ("gf_prop_features", C.c_int, [vp, u64, u64, dbl, vp, i32, vp, vp]),
     ("gf_prop_downsample", C.c_int, [vp, u64, u64, i32, u64, vp, u64, vp]),
     ("gf_flag_harmonics", C.c_int, [vp, u64, C.POINTER(HarmonicContext), C.POINTER(HarmonicOptions), vp, vp]),
+    ("gf_flag_harmonics_device", C.c_int, [vp, u64, C.POINTER(HarmonicContext), C.POINTER(HarmonicOptions), vp,
+                                           vp, i32, vp]),
     ("gf_remove_harmonics", C.c_int, [vp, vp, u64, u64, vp, C.POINTER(u64)]),
 ]
 

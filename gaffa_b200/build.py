@@ -16,7 +16,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libgaffa_b200.so"
-SOURCES = ["host.cpp", "dedisperse.cu", "preprocess.cu", "ffa.cu", "fold.cu", "synth.cu", "filterbank.cu", "proposal.cu", "candidates.cu"]
+SOURCES = ["host.cpp", "dedisperse.cu", "preprocess.cu", "ffa.cu", "fold.cu", "synth.cu", "filterbank.cu", "proposal.cu", "candidates.cu", "harmonics.cu"]
 # gaffa's C++ API (include/gaffa/*.h) over the C ABI: plain C++20 host code
 CXX_SOURCES = ["cxx_api.cpp"]
 CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra", f"-I{ROOT / 'include'}",

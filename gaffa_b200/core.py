@@ -758,17 +758,31 @@ def harmonic_options(max_harmonic: int = 16, denominator_max: int = 5, frequency
                                 dm_distance_max, int(use_snr_consistency), 0, snr_distance_max)
 
 
+# candidate counts from which harmonic flagging runs its pairwise tests on the GPU
+DEVICE_HARMONIC_MIN = 4096
+
+
 def flag_harmonics(candidates: np.ndarray, observation_seconds: float, frequency_low_mhz: float,
-                   frequency_high_mhz: float, options=None) -> tuple[np.ndarray, np.ndarray]:
+                   frequency_high_mhz: float, options=None, device_id: int | None = None) -> tuple[np.ndarray, np.ndarray]:
     """flag_harmonics_cpu (src/gaffa/harmonic.cpp:245-292): the candidates in
-    harmonic ranking order and their relations (HARMONIC_DTYPE)."""
+    harmonic ranking order and their relations (HARMONIC_DTYPE).  The n^2/2
+    pairwise tests run on the GPU (gf_flag_harmonics_device, same decisions)
+    when device_id is given, or from DEVICE_HARMONIC_MIN candidates on."""
     candidates = np.ascontiguousarray(candidates, _lib.CAND_DTYPE)
     ctx = _lib.HarmonicContext(observation_seconds, frequency_low_mhz, frequency_high_mhz)
     opts = options if options is not None else harmonic_options()
     out = np.zeros(len(candidates), _lib.CAND_DTYPE)
     rel = np.zeros(len(candidates), _lib.HARMONIC_DTYPE)
-    check(_lib.lib().gf_flag_harmonics(ptr(candidates), len(candidates), C.byref(ctx), C.byref(opts),
-                                       ptr(out) if len(out) else None, ptr(rel) if len(rel) else None))
+    if device_id is None and len(candidates) >= DEVICE_HARMONIC_MIN and torch.cuda.is_available():
+        device_id = torch.cuda.current_device()
+    if device_id is None:
+        check(_lib.lib().gf_flag_harmonics(ptr(candidates), len(candidates), C.byref(ctx), C.byref(opts),
+                                           ptr(out) if len(out) else None, ptr(rel) if len(rel) else None))
+    else:
+        with torch.cuda.device(device_id):
+            check(_lib.lib().gf_flag_harmonics_device(ptr(candidates), len(candidates), C.byref(ctx), C.byref(opts),
+                                                      ptr(out) if len(out) else None, ptr(rel) if len(rel) else None,
+                                                      device_id, _stream()))
     return out, rel
 
 

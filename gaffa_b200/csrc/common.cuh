@@ -136,6 +136,15 @@ struct PeakTaskInfo {
   double effective_tsamp;
   uint64_t bins, rows;
 };
+struct HarmonicRatio;
+struct HarmonicInput;
+// The pairwise marking of flag_harmonics_cpu (harmonic.cpp:271-289) on the
+// device: parent[c] = the first non-harmonic candidate before c (in ranking
+// order) of which c is a harmonic, or UINT32_MAX.
+void flag_harmonics_on_device(const std::vector<HarmonicInput>& candidates, const std::vector<HarmonicRatio>& ratios,
+                              double observation_seconds, double band, const gf_harmonic_options& options,
+                              int device, void* stream, std::vector<uint32_t>& parent);
+
 // The task table, width trials and device of a single-plan FFA program.
 void ffa_program_peak_tables(const gf_ffa_program* program, std::vector<PeakTaskInfo>& tasks,
                              std::vector<uint64_t>& widths, int& device);

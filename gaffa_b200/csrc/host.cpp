@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "harmonic_math.cuh"
 
 namespace gf {
 
@@ -341,11 +342,6 @@ extern "C" int gf_select_candidates(const gf_peak* peaks, uint64_t n, double tob
 
 namespace {
 
-struct HarmonicRatio {
-  int32_t num, den;
-  double value;
-};
-
 // Reduced ratios n/d (n <= max_harmonic, d <= denominator_max, n != d) by
 // value, then numerator, then denominator; duplicates removed
 // (harmonic.cpp:94-135).
@@ -371,20 +367,6 @@ std::vector<HarmonicRatio> harmonic_ratios(uint64_t max_harmonic, uint64_t denom
   return r;
 }
 
-// The ratio nearest to x: the first with value >= x unless its predecessor
-// is strictly closer (harmonic.cpp:137-163).
-const HarmonicRatio* nearest_ratio(double x, const std::vector<HarmonicRatio>& r) {
-  if (!(x > 0.0) || r.empty()) return nullptr;
-  const auto lo = std::lower_bound(r.begin(), r.end(), x,
-                                   [](const HarmonicRatio& e, double v) { return e.value < v; });
-  const HarmonicRatio* best = lo != r.end() ? &*lo : nullptr;
-  if (lo != r.begin()) {
-    const HarmonicRatio* prev = &*(lo - 1);
-    if (best == nullptr || std::abs(prev->value - x) < std::abs(best->value - x)) best = prev;
-  }
-  return best;
-}
-
 // harmonic.cpp:21-35
 bool harmonic_rank(const gf_candidate& l, const gf_candidate& r) {
   if (l.snr != r.snr) return l.snr > r.snr;
@@ -407,9 +389,40 @@ gf_harmonic_options default_harmonic_options() {
 
 }  // namespace
 
+namespace {
+
+// |1/lo^2 - 1/hi^2| of the band (harmonic.cpp:170-179)
+double harmonic_band(const gf_harmonic_context& ctx) {
+  const double lo = std::min(ctx.frequency_low_mhz, ctx.frequency_high_mhz);
+  const double hi = std::max(ctx.frequency_low_mhz, ctx.frequency_high_mhz);
+  return std::abs(1.0 / (lo * lo) - 1.0 / (hi * hi));
+}
+
+// flag_harmonics_cpu (harmonic.cpp:245-292); device_id >= 0 marks the pairs
+// on that device
+int flag_harmonics(const gf_candidate* candidates, uint64_t n, const gf_harmonic_context* ctx,
+                   const gf_harmonic_options* options, gf_candidate* sorted_out, gf_harmonic_relation* rel,
+                   int device_id, void* stream);
+
+}  // namespace
+
 extern "C" int gf_flag_harmonics(const gf_candidate* candidates, uint64_t n, const gf_harmonic_context* ctx,
                                  const gf_harmonic_options* options, gf_candidate* sorted_out,
                                  gf_harmonic_relation* rel) {
+  return flag_harmonics(candidates, n, ctx, options, sorted_out, rel, -1, nullptr);
+}
+
+extern "C" int gf_flag_harmonics_device(const gf_candidate* candidates, uint64_t n, const gf_harmonic_context* ctx,
+                                        const gf_harmonic_options* options, gf_candidate* sorted_out,
+                                        gf_harmonic_relation* rel, int32_t device_id, void* stream) {
+  return flag_harmonics(candidates, n, ctx, options, sorted_out, rel, device_id < 0 ? 0 : device_id, stream);
+}
+
+namespace {
+
+int flag_harmonics(const gf_candidate* candidates, uint64_t n, const gf_harmonic_context* ctx,
+                   const gf_harmonic_options* options, gf_candidate* sorted_out, gf_harmonic_relation* rel,
+                   int device_id, void* stream) {
   return guarded([&] {
     check_arg(ctx != nullptr, "null argument");
     const gf_harmonic_options o = options ? *options : default_harmonic_options();
@@ -449,47 +462,37 @@ extern "C" int gf_flag_harmonics(const gf_candidate* candidates, uint64_t n, con
       r.denominator = 1;
     }
     const std::vector<HarmonicRatio> ratios = harmonic_ratios(o.max_harmonic, o.denominator_max);
-    const double lo = std::min(ctx->frequency_low_mhz, ctx->frequency_high_mhz);
-    const double hi = std::max(ctx->frequency_low_mhz, ctx->frequency_high_mhz);
-    const double band = std::abs(1.0 / (lo * lo) - 1.0 / (hi * hi));
-    // a candidate already flagged is neither a parent nor re-tested
-    // (harmonic.cpp:271-289)
-    for (uint64_t pi = 0; pi < n; ++pi) {
-      if (rl[pi].is_harmonic) continue;
-      const gf_candidate& p = s[pi];
-      for (uint64_t ci = pi + 1; ci < n; ++ci) {
-        if (rl[ci].is_harmonic) continue;
-        const gf_candidate& c = s[ci];
-        // harmonic.cpp:186-243
-        const HarmonicRatio* hr = nearest_ratio(c.frequency / p.frequency, ratios);
-        if (hr == nullptr) continue;
-        const double ferr = std::abs(c.frequency - p.frequency * hr->value) * ctx->observation_seconds;
-        if (ferr > o.frequency_tolerance_bins) continue;
-        const double phase = ferr / (c.frequency >= p.frequency ? c.duty_cycle : p.duty_cycle);
-        if (phase > o.phase_distance_max) continue;
-        const double delay_s = std::abs(p.dm - c.dm) * 4.148808e3 * band / 1000.0;
-        const double dist = delay_s / std::min(p.period * p.duty_cycle, c.period * c.duty_cycle);
-        if (dist > o.dm_distance_max) continue;
-        const double esnr = static_cast<double>(p.snr) /
-                            std::sqrt(static_cast<double>(hr->num) * static_cast<double>(hr->den));
-        const double sdist = std::abs(static_cast<double>(c.snr) - esnr);
-        if (o.use_snr_consistency && sdist > o.snr_distance_max) continue;
-        gf_harmonic_relation& r = rl[ci];
-        r.is_harmonic = 1;
-        r.parent_index = pi;
-        r.numerator = hr->num;
-        r.denominator = hr->den;
-        r.frequency_error_bins = ferr;
-        r.phase_distance = phase;
-        r.dm_distance = dist;
-        r.expected_snr = esnr;
-        r.snr_distance = sdist;
+    const double band = harmonic_band(*ctx);
+    std::vector<HarmonicInput> in(n);
+    for (uint64_t i = 0; i < n; ++i) in[i] = harmonic_input(s[i]);
+    if (device_id >= 0) {
+      // the pairwise marking on the device; the relations from the same test on the host
+      std::vector<uint32_t> parent(n);
+      flag_harmonics_on_device(in, ratios, ctx->observation_seconds, band, o, device_id, stream, parent);
+      for (uint64_t ci = 0; ci < n; ++ci) {
+        if (parent[ci] == UINT32_MAX) continue;
+        const bool ok = harmonic_test(in[parent[ci]], in[ci], ratios.data(), static_cast<int>(ratios.size()),
+                                      ctx->observation_seconds, band, o, parent[ci], &rl[ci]);
+        if (!ok) raise(GF_ERUNTIME, "device harmonic flagging disagrees with the host test");
+      }
+    } else {
+      // a candidate already flagged is neither a parent nor re-tested
+      // (harmonic.cpp:271-289)
+      for (uint64_t pi = 0; pi < n; ++pi) {
+        if (rl[pi].is_harmonic) continue;
+        for (uint64_t ci = pi + 1; ci < n; ++ci) {
+          if (rl[ci].is_harmonic) continue;
+          harmonic_test(in[pi], in[ci], ratios.data(), static_cast<int>(ratios.size()), ctx->observation_seconds,
+                        band, o, pi, &rl[ci]);
+        }
       }
     }
     std::memcpy(sorted_out, s.data(), n * sizeof(gf_candidate));
     std::memcpy(rel, rl.data(), n * sizeof(gf_harmonic_relation));
   });
 }
+
+}  // namespace
 
 extern "C" int gf_remove_harmonics(const gf_candidate* sorted, const gf_harmonic_relation* rel, uint64_t n,
                                    uint64_t max_candidates, gf_candidate* out, uint64_t* nout) {

@@ -551,6 +551,17 @@ int gf_flag_harmonics(const gf_candidate* candidates, uint64_t n,
                       const gf_harmonic_options* options,
                       gf_candidate* sorted_out,
                       gf_harmonic_relation* relations_out);
+/* The same flagging with the pairwise tests on a device: for lists of 10^4+
+ * candidates (the n^2 / 2 tests of harmonic.cpp:271-289 take minutes on a
+ * CPU at 10^5).  The decisions use the same FP64 expressions with explicit
+ * rounding, so outputs equal gf_flag_harmonics; host in, host out,
+ * synchronous on `stream`. */
+int gf_flag_harmonics_device(const gf_candidate* candidates, uint64_t n,
+                             const gf_harmonic_context* context,
+                             const gf_harmonic_options* options,
+                             gf_candidate* sorted_out,
+                             gf_harmonic_relation* relations_out,
+                             int32_t device_id, void* stream);
 
 /* Replaces remove_harmonics_cpu, src/gaffa/harmonic.cpp:294-309: the
  * non-harmonic candidates in order, at most max_candidates (0 = all). */

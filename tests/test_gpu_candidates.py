@@ -70,3 +70,61 @@ def test_device_selection_equals_host_selection_under_every_option(seed):
         got = core.select_candidates_device(prog, allrec, segments, 5.0, 0.25, tobs, radius, dm_radius, across, cap)
         assert len(got) == len(want) > 0, (radius, dm_radius, across, cap)
         assert np.array_equal(got, want), (radius, dm_radius, across, cap)
+
+
+def _synthetic_candidates(n, seed):
+    """n candidates over 0.1-10 Hz with planted harmonic families (n/m
+    multiples of fundamentals within a fraction of a Fourier bin, nearby DMs)
+    and noise candidates, ties in S/N and peak counts included."""
+    from gaffa_b200 import _lib
+    rng = np.random.default_rng(seed)
+    tobs = 300.0
+    c = np.zeros(n, _lib.CAND_DTYPE)
+    nf = n // 8
+    f0 = rng.uniform(0.1, 1.0, nf)
+    freq = np.empty(n)
+    freq[:nf] = f0
+    k = np.arange(nf, n)
+    num = rng.integers(1, 17, len(k))
+    den = rng.integers(1, 6, len(k))
+    base = f0[rng.integers(0, nf, len(k))]
+    harm = rng.random(len(k)) < 0.6
+    freq[nf:] = np.where(harm, base * num / den + rng.normal(0, 0.3 / tobs, len(k)), rng.uniform(0.1, 10.0, len(k)))
+    freq = np.abs(freq) + 1e-3
+    c["frequency"] = freq
+    c["period"] = 1.0 / freq
+    c["duty_cycle"] = rng.uniform(0.01, 0.1, n)
+    c["dm_index"] = rng.integers(0, 2048, n)
+    c["dm"] = c["dm_index"] * 0.4885
+    c["snr"] = np.round(rng.uniform(8, 30, n), 1).astype(np.float32)        # many S/N ties
+    c["peak_count"] = rng.integers(1, 50, n)
+    c["width"] = 4
+    return c, tobs
+
+
+@pytest.mark.parametrize("n,seed", [(39, 0), (3000, 1), (20000, 2)])
+def test_device_harmonic_flagging_equals_host(n, seed):
+    from gaffa_b200 import core
+    if n == 39:
+        g = np.load(Path(__file__).resolve().parent / "golden" / "ref_plain_end_to_end.npz")
+        cands, tobs = g["candidates"], 2 ** 18 * 64e-6
+        lo, hi = 1200.0, 1500.0
+    else:
+        cands, tobs = _synthetic_candidates(n, seed)
+        lo, hi = 1100.0, 1700.0
+    host = core.flag_harmonics(cands, tobs, lo, hi, device_id=None) if n < core.DEVICE_HARMONIC_MIN else None
+    if host is None:
+        from gaffa_b200 import _lib
+        import ctypes as C
+        ctx = _lib.HarmonicContext(tobs, lo, hi)
+        opts = core.harmonic_options()
+        out = np.zeros(n, _lib.CAND_DTYPE)
+        rel = np.zeros(n, _lib.HARMONIC_DTYPE)
+        _lib.check(_lib.lib().gf_flag_harmonics(_lib.ptr(np.ascontiguousarray(cands)), n, C.byref(ctx),
+                                                C.byref(opts), _lib.ptr(out), _lib.ptr(rel)))
+        host = (out, rel)
+    dev = core.flag_harmonics(cands, tobs, lo, hi, device_id=0)
+    assert np.array_equal(dev[0], host[0])
+    assert np.array_equal(dev[1], host[1])
+    if n > 39:
+        assert dev[1]["is_harmonic"].sum() > n // 10      # the planted families are found
