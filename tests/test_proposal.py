@@ -102,14 +102,19 @@ def test_cuda_forward_and_gradients_match_oracle():
     bs = [b.cpu().double().numpy() for b in net.b]
     ref = po.loss_and_grads(feat.float().cpu().numpy(), ws, bs, net.wh.cpu().double().numpy(),
                             net.bh.cpu().double().numpy(), labels.cpu().double().numpy(), 7.0, OCT)
-    np.testing.assert_allclose(logits.cpu().numpy(), ref[5], rtol=2e-2, atol=2e-2)
-    assert abs(loss - ref[0]) < 1e-2 * abs(ref[0])
+    # The oracle rounds to bf16 where the kernels do; what remains is the FP32
+    # summation order, which can move a value across a bf16 rounding
+    # boundary.  Observed over six seeds on a B200: logits within 1.5e-4,
+    # loss within 1.5e-5 relative, gradients within 1.0e-3 of their norm
+    # (first conv layer; the others within 3.3e-4).  Bounds: 3x those.
+    np.testing.assert_allclose(logits.cpu().numpy(), ref[5], rtol=5e-4, atol=5e-4)
+    assert abs(loss - ref[0]) < 5e-5 * abs(ref[0])
     nl = len(proposal.LAYERS)
     pairs = list(zip(grads[:nl], ref[1])) + list(zip(grads[nl:2 * nl], ref[2])) + [(grads[2 * nl], ref[3]),
                                                                                      (grads[2 * nl + 1], ref[4])]
     for g, r in pairs:
         g = g.cpu().double().numpy()
-        assert np.linalg.norm(g - r) <= 3e-2 * np.linalg.norm(r) + 1e-9
+        assert np.linalg.norm(g - r) <= 3e-3 * np.linalg.norm(r) + 1e-9
 
 
 @pytest.mark.gpu
