@@ -352,32 +352,6 @@ struct DetectArgs {
   unsigned long long* counters;
 };
 
-// Per-row statistics kept after a row's prefix sums (at c[bins + max_width +
-// 1 ...]): its three largest samples and the sum of |samples|.
-constexpr uint32_t kRowStats = 4;
-
-// Whether no phase of width tr.width can reach the threshold on this row:
-// the boxcar sum of w samples is at most the sum of the row's w largest
-// samples (t1 + t2 + (w - 2) t3), the FP32 prefix sums move a computed
-// boxcar by at most E = 4 (bins + 64) u sum|x| (first-order bound of the
-// sequential sums, u = 2^-24), and the FP32 S/N expression is within a
-// relative 1e-5 of its terms.  The bound is evaluated in FP64; when it stays
-// below the threshold the width is skipped, which removes no peak (the scan
-// would find none).  On noise rows it skips ~6 of 7 widths.
-__device__ __forceinline__ bool width_cannot_pass(const TrialDev& tr, float t1, float t2, float t3, float sabs,
-                                                  float psum, float inv_stdnoise, float threshold, uint32_t bins) {
-  const double w = static_cast<double>(tr.width);
-  double top = static_cast<double>(t1);
-  if (tr.width >= 2) top += static_cast<double>(t2);
-  if (tr.width >= 3) top += (w - 2.0) * static_cast<double>(t3);
-  const double err = 4.0 * static_cast<double>(bins + 64) * 5.9604644775390625e-8 * static_cast<double>(sabs);
-  const double hb = static_cast<double>(__fadd_rn(tr.height, tr.baseline));
-  const double a = hb * (top + err), b = static_cast<double>(tr.baseline) * static_cast<double>(psum);
-  const double inv = static_cast<double>(inv_stdnoise);
-  const double bound = (a - b) * inv + 1e-5 * (fabs(a) + fabs(b)) * inv + 1e-6;
-  return bound < static_cast<double>(threshold);
-}
-
 // order-preserving map of finite floats to unsigned keys (for redux.sync)
 __device__ __forceinline__ uint32_t float_key(float f) {
   const uint32_t u = __float_as_uint(f);
@@ -403,17 +377,6 @@ __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, u
     const float* prof = rows + threadIdx.x * pitch;
     float* c = cp + threadIdx.x * cp_pitch;
     float acc = 0.0f;
-    // the row's three largest samples and sum of |samples| (width_cannot_pass);
-    // these chains run beside the prefix's add chain
-    float t1 = -INFINITY, t2 = -INFINITY, t3 = -INFINITY, sabs = 0.0f;
-    auto keep = [&](float v) {
-      const float lo1 = fminf(t1, v);
-      t1 = fmaxf(t1, v);
-      const float lo2 = fminf(t2, lo1);
-      t2 = fmaxf(t2, lo1);
-      t3 = fmaxf(t3, lo2);
-      sabs = sabs + fabsf(v);
-    };
     c[0] = 0.0f;
     // loads of the next 8 samples overlap the current 8-add chain
     float cur[8], nxt[8];
@@ -427,7 +390,6 @@ __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, u
       for (int j = 0; j < 8; ++j) {
         acc = __fadd_rn(acc, cur[j]);
         c[i + j + 1] = acc;
-        keep(cur[j]);
       }
 #pragma unroll
       for (int j = 0; j < 8; ++j) cur[j] = nxt[j];
@@ -435,17 +397,11 @@ __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, u
     for (uint32_t i = nfull; i < bins; ++i) {
       acc = __fadd_rn(acc, prof[i]);
       c[i + 1] = acc;
-      keep(prof[i]);
     }
     for (uint32_t i = 0; i < a.max_width; ++i) {
       acc = __fadd_rn(acc, prof[i]);
       c[bins + i + 1] = acc;
     }
-    float* st = c + bins + a.max_width + 1;
-    st[0] = t1;
-    st[1] = t2;
-    st[2] = t3;
-    st[3] = sabs;
   }
   __syncthreads();
   const bool last_ok = lane + 32u * (NB - 1) < bins;
@@ -455,12 +411,8 @@ __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, u
 #pragma unroll
     for (int i = 0; i < NB; ++i) base[i] = (i < NB - 1 || last_ok) ? c[32 * i] : 0.0f;
     const float psum = cp[r * cp_pitch + bins];
-    const float* st = cp + r * cp_pitch + bins + a.max_width + 1;
-    const float t1 = st[0], t2 = st[1], t3 = st[2], sabs = st[3];
     for (uint32_t k = 0; k < a.ntrials; ++k) {
       const TrialDev tr = a.trials[k];
-      // warp-uniform: the same row statistics in every lane
-      if (width_cannot_pass(tr, t1, t2, t3, sabs, psum, a.inv_stdnoise, a.threshold, bins)) continue;
       const float* cw = c + tr.width;
       float best = -INFINITY;
 #pragma unroll
@@ -659,7 +611,7 @@ __global__ void __launch_bounds__(kThreads, 2) ffa_search_kernel(SearchParams p)
     const float* input = base + series * stride + t.prep_offset;
     const uint32_t bins = t.bins;
     const DetectArgs da = make_detect(p, t, series, task);
-    const uint32_t cp_pitch = (bins + t.max_width + kRowStats + 2) | 1u;
+    const uint32_t cp_pitch = (bins + t.max_width + 2) | 1u;
     const uint32_t dS = t.split_depth;
     if (dS == 0) {
       // whole task on chip: levels below the root, then root rows in batches
@@ -1130,7 +1082,7 @@ std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& spe
     // R + 3 (2^K - 1) rows at the bottom of a column
     while (g.levels > 1 && static_cast<int>(rows) - 3 * ((1 << g.levels) - 1) < 8) --g.levels;
     g.block_rows = rows - 3 * ((1u << g.levels) - 1);
-    const uint32_t cp_pitch = (cap + P->max_width + kRowStats + 2) | 1u;
+    const uint32_t cp_pitch = (cap + P->max_width + 2) | 1u;
     g.cp_rows = (rows * g.pitch) / cp_pitch;
     g.final_rows = std::min<uint32_t>(g.block_rows, g.cp_rows);
     check_arg(g.final_rows >= 1 && g.block_rows >= 1, "FFA bins too large for the shared-memory tiles");
