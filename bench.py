@@ -61,6 +61,8 @@ def parse_args():
                     help="fraction of DM windows searched (default: the shipped model's)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven-workload measurement")
     ap.add_argument("--batched-observations", type=int, default=12)
+    ap.add_argument("--batched-configured", action="store_true",
+                    help="also run the batched workload at its configured laws (64 observations, ~15 minutes)")
     ap.add_argument("--no-wide-subband", action="store_true",
                     help="skip the wide-range subband measurement at its configured size")
     return ap.parse_args()
@@ -418,6 +420,72 @@ def batched_measurement(nobs: int, device_id: int, case: str = "reduced") -> dic
             "tuned_dedispersion_shapes": tuner.cache, "case": case, "laws": BATCHED_CASES[case]}
 
 
+def batched_configured_measurement(device_id: int, nobs: int = 64, memory_fraction: float = 0.3) -> dict:
+    """The batched uneven workload at its configured laws: 64 observations,
+    channels from {1024, 2048, 4096}, lengths log-uniform over 2^20-2^23,
+    256-4096 DM trials, own FFA period ranges, 0-4 pulsars each (631 GB of
+    raw input in all).  The observations are searched in consecutive
+    sub-batches whose filterbanks and staging buffers fit memory_fraction of
+    the free HBM; each sub-batch is generated on the device, set up (launch
+    shapes tuned, waves captured as CUDA graphs) outside the timing, then
+    searched once by BatchSearch from its device filterbanks and once by
+    DmSearch one observation after another.  Reports both throughputs, the
+    speed-up, kernel launches per wave and whether every result is identical."""
+    import torch
+    from gaffa_b200 import batch, configs, core, search
+    cs = configs.batched_uneven(seed=0, nobs=nobs)
+    free = torch.cuda.mem_get_info(device_id)[0]
+    budget = int(free * memory_fraction)
+    groups, cur, used = [], [], 0
+    for c in cs:
+        need = 2 * c.obs.nchans * c.obs.nsamples
+        if cur and used + need > budget:
+            groups.append(cur)
+            cur, used = [], 0
+        cur.append(c)
+        used += need
+    if cur:
+        groups.append(cur)
+    tuner = batch.Autotuner()
+    t_batched = t_seq = 0.0
+    units = 0
+    same = True
+    launches, waves = [], 0
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - a, out
+
+    for sub in groups:
+        data = [core.synth_generate(c.obs, device_id=device_id) for c in sub]
+        bs = batch.BatchSearch(sub, device_id=device_id, tuner=tuner)
+        bs.run(data)                                   # tunes shapes, builds and captures the waves
+        dt, got = timed(lambda: bs.run(data))
+        t_batched += dt
+        units += sum(c.ndm * dd.nout for c, dd in zip(sub, bs.dd))
+        launches.append(bs.kernel_launches_per_run)
+        waves += len(bs.waves)
+        del bs
+        torch.cuda.empty_cache()
+        for c, x, g in zip(sub, data, got):
+            ds = search.from_config(c, device_id=device_id)
+            dt, want = timed(lambda: ds.run(x))
+            t_seq += dt
+            same = same and np.array_equal(g.peaks, want.peaks) and np.array_equal(g.candidates, want.candidates)
+            del ds
+        del data
+        torch.cuda.empty_cache()
+    return {"value": units / t_batched, "unit": UNIT, "observations": nobs, "sub_batches": len(groups),
+            "waves": waves, "dm_trial_samples": units, "seconds": t_batched, "sequential_seconds": t_seq,
+            "sequential_value": units / t_seq, "speedup_vs_sequential": t_seq / t_batched,
+            "kernel_launches_per_sub_batch": launches, "identical_to_sequential": bool(same),
+            "tuned_dedispersion_shapes": tuner.cache,
+            "laws": "configs.batched_uneven: channels {1024, 2048, 4096}, 2^20-2^23 samples, 256-4096 DMs"}
+
+
 def wide_subband_measurement(device_id: int) -> dict:
     """The wide-range subband workload at its configured size (2-bit, 4096
     channels over 300-400 MHz, 2^22 samples, 64 subbands, nominal DMs every
@@ -504,6 +572,9 @@ def main():
         batched_small = batched_measurement(64, local, "small")
     if rank == 0 and world == 1 and not args.no_wide_subband and args.workload != "wide_subband":
         wide = wide_subband_measurement(local)
+    batched_configured = None
+    if rank == 0 and world == 1 and args.batched_configured:
+        batched_configured = batched_configured_measurement(local)
     cfg = workload(args, rank)
     obs = cfg.obs
     raw = core.synth_generate(obs, device_id=local)          # device-resident filterbank
@@ -635,6 +706,7 @@ def main():
             "batched": batched,
             "batched_small": batched_small,
             "wide_subband": wide,
+            "batched_configured": batched_configured,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -176,6 +176,7 @@ _SIGNATURES = [
     ("gf_dedisp_stage", C.c_int, [vp, vp, vp, vp]),
     ("gf_dedisp_stage_from_host", C.c_int, [vp, vp, vp, vp, u64, vp]),
     ("gf_dedisp_run", C.c_int, [vp, vp, u64, u64, vp, u64, vp, vp]),
+    ("gf_dedisp_check", C.c_int, [vp, vp]),
     ("gf_preprocess_info_get", C.c_int, [C.POINTER(PreprocessDesc), C.POINTER(PreprocessInfo)]),
     ("gf_preprocess_inplace", C.c_int, [C.POINTER(PreprocessDesc), vp, i32, u64, u64, vp, vp, vp, vp]),
     ("gf_normalise", C.c_int, [vp, u64, u64, u64, vp, vp]),

@@ -306,6 +306,8 @@ class BatchSearch:
                 parts[pc.obs].append(peaks[member == m])
         for pre in self.pre:
             pre.synchronize()
+        for dd in self.dd:
+            dd.check()
         t2 = time.perf_counter()
         results = [self._finish(i, c, parts[i]) for i, c in enumerate(self.configs)]
         t3 = time.perf_counter()
@@ -331,6 +333,7 @@ class BatchSearch:
             b0 = dm_index // 8 * 8
             cnt = min(8, c.ndm - b0)
             series = dd.run(self.staged[i], b0, cnt, out_stride=self.strides[i])
+            dd.check()
             prof, expo = core.fold_time_series(series[dm_index - b0, : dd.nout], period, o.tsamp, c.fold_nbin)
         return SearchResult(peaks=peaks, candidates=cands, fold_profile=prof, fold_exposure=expo, nout=dd.nout,
                             ndm=c.ndm, timings={}, gpu_launches=0, ranked=ranked, harmonics=rel,

@@ -208,6 +208,12 @@ class DedispersionProgram:
                                            ptr(workspace), _stream(stream)))
         return out.view(-1)[: dm_count * out_stride].view(dm_count, out_stride)
 
+    def check(self, stream=None) -> None:
+        """Synchronises the stream and raises if a launch of this program gave
+        up waiting for a shared-memory copy stage (gf_dedisp_check)."""
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_dedisp_check(self._h, _stream(stream)))
+
 
 class DedispersionBatch:
     """Many brute-force (program, staged input, DM range, output) items of

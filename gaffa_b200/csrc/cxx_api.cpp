@@ -144,7 +144,7 @@ gaffa::CudaDedispersedResult<std::uint32_t> dedisperse_u8(gaffa::HostSampleView<
   check(gf_dedisp_run(program.handle, staged.data(), 0, ndm, result.data.data(), info.nout, workspace.data(),
                       nullptr),
         "dedisperse_cuda");
-  check_cuda(cudaStreamSynchronize(nullptr), "dedisperse_cuda");
+  check(gf_dedisp_check(program.handle, nullptr), "dedisperse_cuda");  // synchronises
   return result;
 }
 

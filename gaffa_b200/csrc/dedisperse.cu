@@ -11,20 +11,26 @@
 //
 // Kernel.  One CTA = a block of DB DMs x a time tile; each warp owns one DM and
 // 1008 consecutive output samples (252 output words of 4 samples).  The CTA
-// streams channel chunks: for each channel it copies the window
-// [t0 + base, t0 + base + RS) (base = delay of the block's first DM rounded down
-// to 16) into shared memory with 16-byte cp.async copies, double-buffered so
-// chunk k+1 lands while chunk k is summed.  DM blocks are the fastest grid
-// index, so the CTAs resident at one time cover a few time tiles of every DM
-// block of the launch and read each input window from L2.  A warp reads its DM's shifted
+// streams channel chunks through a ring of 2-4 shared-memory stages: for each
+// channel of a chunk one bulk copy (cp.async.bulk, completion counted in bytes
+// on the stage's mbarrier) brings the window [t0 + base, t0 + base + RS)
+// (base = delay of the block's first DM rounded down to 16), and one more per
+// DM its gather records.  Warps wait on the stage's barrier, sum, and release
+// the stage with an acquire-release counter; the last warp to release it
+// issues the copies of the chunk `stages` ahead into it.  No CTA-wide barrier
+// runs per chunk, so warps drift apart by up to `stages` chunks.  DM blocks
+// are the fastest grid index, so the CTAs resident at one time cover a few
+// time tiles of every DM block of the launch and read each input window from
+// L2.  A warp reads its DM's shifted
 // window as aligned 32-bit words: the delay offset off = d - base splits into a
 // word offset q = off >> 2 and a byte class s = off & 3.  The host sorts each
 // warp's channels by class, so the class is static inside the loop: a word
 // holds 4 consecutive input bytes, which are split into even/odd byte pairs
-// (LOP3 and PRMT) and accumulated in 16-bit lanes (IADD3 folds two channels).
-// Per 256 channels the 16-bit lanes are flushed into 32-bit sums, realigning
-// class s by s bytes with one lane shuffle.  Lanes read consecutive words, so
-// every LDS.32 is conflict-free.
+// (LOP3 and PRMT) and accumulated in 16-bit lanes by IMAD; a class with an
+// odd channel count ends with one single-channel step.  Per 256 channels the
+// 16-bit lanes are flushed into 32-bit sums, realigning class s by s bytes
+// with one lane shuffle.  Lanes read consecutive words, so every LDS.32 is
+// conflict-free.
 #include "common.cuh"
 
 #include <algorithm>
@@ -56,6 +62,11 @@ constexpr int kOutWords = 32 * kWords - 4;      // 252 output words per warp
 constexpr int kWarpSamples = 4 * kOutWords;     // 1008 samples per warp
 constexpr int kFlushChannels = 256;             // 16-bit lanes hold 256 x 255
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kMaxStages = 4;
+// A stage whose copies have not landed after this many SM cycles (~2 s) is
+// given up: the CTA sets GF_STATUS_PIPELINE in the program's status word
+// (read by gf_dedisp_check) and returns.
+constexpr long long kWaitCycles = 4000000000ll;
 
 struct BytesParams {
   const uint8_t* in;         // group 0, row 0 of the launch
@@ -87,7 +98,16 @@ struct BytesParams {
   uint64_t out_group_rows;
   uint64_t nout;             // valid output samples
   uint32_t grid_x;           // CTAs per group (grid x)
-  uint32_t reserved;
+  int stages;                // shared-memory stages in the copy ring (2-4)
+  uint32_t stage_bytes;      // chunk_rows * row_bytes + dms_per_cta * record_words * 4
+  uint32_t* status;          // GF_STATUS_PIPELINE when a stage wait gives up
+};
+
+// Copy-ring state in static shared memory.
+struct PipeShared {
+  uint64_t full[kMaxStages];      // one phase per use of the stage: 32 arrivals + the copied bytes
+  uint32_t released[kMaxStages];  // warps done with the stage's current chunk
+  uint32_t failed;                // a wait of this CTA gave up
 };
 
 __device__ __forceinline__ uint32_t lo16(uint32_t v) { return v & 0xffffu; }
@@ -147,17 +167,153 @@ __device__ __forceinline__ void accumulate_class(const uint32_t* __restrict__ sm
   pos += npairs;
 }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+// The last entry of a class with an odd channel count (low half of its word).
+template <int S>
+__device__ __forceinline__ void accumulate_single(const uint32_t* __restrict__ smem_words, uint32_t entry,
+                                                  int lane_word, uint32_t (&e)[kWords], uint32_t (&o)[kWords],
+                                                  uint32_t one) {
+  const uint32_t* a = smem_words + (entry & 0xffffu) + lane_word;
+#pragma unroll
+  for (int m = 0; m < kWords; ++m) {
+    const uint32_t w = a[32 * m];
+    e[m] = (w & 0x00ff00ffu) * one + e[m];
+    o[m] = __byte_perm(w, 0u, 0x4341) * one + o[m];
+  }
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// A class's entries: npairs = count / 2 pairs, then the odd one out.
+template <int S>
+__device__ __forceinline__ void accumulate_entries(const uint32_t* __restrict__ smem_words,
+                                                   const uint32_t* __restrict__ rec, int& pos, uint32_t count,
+                                                   int lane_word, uint32_t (&e)[kWords], uint32_t (&o)[kWords],
+                                                   uint32_t one) {
+  accumulate_class<S>(smem_words, rec, pos, static_cast<int>(count >> 1), lane_word, e, o, one);
+  if (count & 1u) {
+    accumulate_single<S>(smem_words, rec[pos], lane_word, e, o, one);
+    ++pos;
+  }
+}
+
+// -- copy ring primitives (PTX ISA 8.x: mbarrier, cp.async.bulk) -------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile(
+      "{\n\t.reg .b64 state;\n\t"
+      "mbarrier.arrive.release.cta.shared::cta.b64 state, [%0];\n}\n" ::"r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Global -> shared copy of `bytes` (a multiple of 16, both addresses 16-byte
+// aligned) completing on `bar`.  No multicast: the source is this GPU's memory.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ uint32_t release_stage(uint32_t* counter) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], 1;\n" : "=r"(old) : "r"(smem_u32(counter)) : "memory");
+  return old;
+}
+// Waits for phase `parity` of `bar`; false when it gave up (this CTA's
+// failure flag, another CTA's status bit, or kWaitCycles).
+__device__ __forceinline__ bool wait_stage(uint64_t* bar, uint32_t parity, const PipeShared& ps,
+                                        const uint32_t* status) {
+  const long long start = clock64();
+  for (uint32_t i = 0;; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*reinterpret_cast<const volatile uint32_t*>(&ps.failed)) return false;
+    if ((i & 255u) == 255u && (*reinterpret_cast<const volatile uint32_t*>(status) & GF_STATUS_PIPELINE))
+      return false;
+    if (clock64() - start > kWaitCycles) return false;
+  }
+}
+
+// The calling warp stages chunk k of CTA (group, block, t0) into stage s:
+// lane r copies channel rows r and r + 32 (bulk below the last 16-byte
+// boundary of the valid samples, by hand with zeros past them), lanes
+// d < dms_per_cta the records of DM d.  The stage's barrier completes after
+// the 32 lane arrivals and the bytes that lane 0 announced.  Runs once per
+// chunk; rows are taken one at a time (row windows recomputed in the second
+// pass) to keep its registers few next to the summing loop's accumulators.
+__device__ __forceinline__ uint32_t row_bulk_bytes(const BytesParams& p, uint64_t t_row) {
+  const uint64_t bulk_end = p.in_valid & ~15ull;
+  return t_row < bulk_end ? static_cast<uint32_t>(umin64(p.row_bytes, bulk_end - t_row)) : 0u;
+}
+
+__device__ __forceinline__ void issue_chunk(const BytesParams& p, PipeShared& ps, uint8_t* smem, int k, int s,
+                                            int group, int block, uint64_t t0, int dm_limit, int group_rows) {
+  const int lane = threadIdx.x & 31;
+  const int32_t* base = p.base + group * p.base_group_stride + static_cast<uint64_t>(block) * p.rows_per_group;
+  const int row0 = k * p.chunk_rows;
+  const int nrows = min(p.chunk_rows, group_rows - row0);
+  const int dl = block * p.dms_per_cta + lane;
+  const bool rec_copy = lane < p.dms_per_cta && dl < dm_limit;
+  uint32_t bytes = rec_copy ? static_cast<uint32_t>(p.record_words) * 4u : 0u;
+#pragma unroll 1
+  for (int r = lane; r < nrows; r += 32) bytes += row_bulk_bytes(p, t0 + static_cast<uint64_t>(base[row0 + r]));
+  const uint32_t total = __reduce_add_sync(kFull, bytes);
+  if (lane == 0) mbar_expect_tx(&ps.full[s], total);
+  __syncwarp();
+  fence_proxy_async_smem();  // earlier generic accesses of the stage before the copies' writes
+  uint8_t* rows = smem + static_cast<uint32_t>(s) * p.stage_bytes;
+#pragma unroll 1
+  for (int r = lane; r < nrows; r += 32) {
+    const uint64_t t_row = t0 + static_cast<uint64_t>(base[row0 + r]);
+    const uint32_t nbulk = row_bulk_bytes(p, t_row);
+    const uint8_t* src = p.in + group * p.in_group_stride + static_cast<uint64_t>(row0 + r) * p.in_row_stride;
+    uint8_t* dst = rows + r * p.row_bytes;
+    if (nbulk) bulk_copy(dst, src + t_row, nbulk, &ps.full[s]);
+#pragma unroll 1
+    for (uint32_t b = nbulk; b < static_cast<uint32_t>(p.row_bytes); b += 16) {
+      const uint64_t t = t_row + b;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (t < p.in_valid) {
+        uint8_t tmp[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) tmp[q] = (t + q < p.in_valid) ? src[t + q] : 0;
+        memcpy(&v, tmp, 16);
+      }
+      *reinterpret_cast<uint4*>(dst + b) = v;
+    }
+  }
+  if (rec_copy)
+    bulk_copy(reinterpret_cast<uint32_t*>(rows + static_cast<uint32_t>(p.chunk_rows) * p.row_bytes) +
+                  lane * p.record_words,
+              p.records + group * p.rec_group_stride + dl * p.rec_dm_stride +
+                  static_cast<uint64_t>(k) * p.record_words,
+              static_cast<uint32_t>(p.record_words) * 4u, &ps.full[s]);
+  mbar_arrive(&ps.full[s]);
+}
 
 // One CTA of a bytes launch: CTA bx of group `group` (grid x and z).
 template <typename OutT>
-__device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int group, uint8_t* smem) {
+__device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int group, uint8_t* smem,
+                                          PipeShared& ps) {
   // DM block fastest: the CTAs resident at once share their input windows in L2
   const int block = static_cast<int>(bx % static_cast<unsigned>(p.nblocks));
   const uint64_t t0 = static_cast<uint64_t>(bx / static_cast<unsigned>(p.nblocks)) * p.cta_samples;
@@ -170,58 +326,20 @@ __device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int
   const bool active = dm_sub < p.dms_per_cta && dm_local < dm_limit;
 
   const int group_rows = min(p.rows_per_group, p.total_rows - group * p.rows_per_group);
-  // two stage buffers: chunk rows + a zero row, then the chunk's records
-  const uint32_t rows_bytes = static_cast<uint32_t>(p.chunk_rows + 1) * p.row_bytes;
-  const uint32_t buf_bytes = rows_bytes + static_cast<uint32_t>(p.dms_per_cta * p.record_words) * 4u;
-  const uint8_t* in_group = p.in + group * p.in_group_stride;
-  const int32_t* base = p.base + group * p.base_group_stride + static_cast<uint64_t>(block) * p.rows_per_group;
+  // a stage: chunk_rows channel windows, then the chunk's records of every DM
+  const uint32_t rows_bytes = static_cast<uint32_t>(p.chunk_rows) * p.row_bytes;
 
-  // zero rows (class padding entries point at them)
-  for (int i = threadIdx.x; i < 2 * (p.row_bytes / 16); i += kThreads) {
-    const int b = i / (p.row_bytes / 16), v = i % (p.row_bytes / 16);
-    reinterpret_cast<uint4*>(smem + b * buf_bytes + p.chunk_rows * p.row_bytes)[v] = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < p.stages; ++s) {
+      mbar_init(&ps.full[s], 32);
+      ps.released[s] = 0;
+    }
+    // another CTA of the launch gave up: do nothing
+    ps.failed = (*reinterpret_cast<const volatile uint32_t*>(p.status) & GF_STATUS_PIPELINE) ? 1u : 0u;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-
-  // chunk k's channel windows and records into buffer b (async where in range)
-  auto stage = [&](int k, int b) {
-    uint8_t* rows = smem + b * buf_bytes;
-    uint32_t* rec_smem = reinterpret_cast<uint32_t*>(rows + rows_bytes);
-    const int row0 = k * p.chunk_rows;
-    const int nrows = min(p.chunk_rows, group_rows - row0);
-    // a warp per channel row, lanes over its 16-byte vectors
-    const int vecs_per_row = p.row_bytes / 16;
-    for (int r = warp; r < nrows; r += kWarps) {
-      const uint64_t t_row = t0 + static_cast<uint64_t>(base[row0 + r]);
-      const uint8_t* src_row = in_group + static_cast<uint64_t>(row0 + r) * p.in_row_stride + t_row;
-      uint8_t* dst_row = rows + r * p.row_bytes;
-      for (int v = lane; v < vecs_per_row; v += 32) {
-        const uint64_t t = t_row + 16ull * v;
-        if (t + 16 <= p.in_valid) {
-          cp_async16(dst_row + 16 * v, src_row + 16 * v);
-        } else {
-          uint8_t tmp[16];
-#pragma unroll
-          for (int j = 0; j < 16; ++j) tmp[j] = (t + j < p.in_valid) ? src_row[16 * v + j] : 0;
-          uint4 val;
-          memcpy(&val, tmp, 16);
-          *reinterpret_cast<uint4*>(dst_row + 16 * v) = val;
-        }
-      }
-    }
-    const int vecs_per_rec = p.record_words / 4;
-    for (int i = threadIdx.x; i < p.dms_per_cta * vecs_per_rec; i += kThreads) {
-      const int d = i / vecs_per_rec;
-      const int w = 4 * (i - d * vecs_per_rec);
-      const int dl = block * p.dms_per_cta + d;
-      uint32_t* dst = rec_smem + d * p.record_words + w;
-      if (dl < dm_limit) {
-        cp_async16(dst, p.records + group * p.rec_group_stride + dl * p.rec_dm_stride +
-                            static_cast<uint64_t>(k) * p.record_words + w);
-      } else {
-        *reinterpret_cast<uint4*>(dst) = make_uint4(0, 0, 0, 0);
-      }
-    }
-  };
+  __syncthreads();
+  if (ps.failed) return;
 
   uint32_t e[4][kWords], o[4][kWords], acc[kWords][4];
 #pragma unroll
@@ -234,27 +352,26 @@ __device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int
   const int lane_word = sub * kOutWords + lane;
   const int chunks_per_flush = kFlushChannels / p.chunk_rows;
 
-  stage(0, 0);
-  cp_async_commit();
+  if (warp == 0)
+    for (int k = 0; k < min(p.stages, p.nchunks); ++k) issue_chunk(p, ps, smem, k, k, group, block, t0, dm_limit, group_rows);
+  int s = 0;
+  uint32_t parity = 0;
+  bool ok = true;
   for (int k = 0; k < p.nchunks; ++k) {
-    if (k + 1 < p.nchunks) {
-      stage(k + 1, (k + 1) & 1);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+    if (!wait_stage(&ps.full[s], parity, ps, p.status)) {
+      ok = false;
+      break;
     }
-    __syncthreads();
     if (active) {
-      const uint8_t* rows = smem + (k & 1) * buf_bytes;
+      const uint8_t* rows = smem + static_cast<uint32_t>(s) * p.stage_bytes;
       const uint32_t* smem_words = reinterpret_cast<const uint32_t*>(rows);
       const uint32_t* rec = reinterpret_cast<const uint32_t*>(rows + rows_bytes) + dm_sub * p.record_words;
       const uint32_t counts = rec[0];
       int pos = 1;
-      accumulate_class<0>(smem_words, rec, pos, (counts & 0xffu) >> 1, lane_word, e[0], o[0], p.one);
-      accumulate_class<1>(smem_words, rec, pos, ((counts >> 8) & 0xffu) >> 1, lane_word, e[1], o[1], p.one);
-      accumulate_class<2>(smem_words, rec, pos, ((counts >> 16) & 0xffu) >> 1, lane_word, e[2], o[2], p.one);
-      accumulate_class<3>(smem_words, rec, pos, (counts >> 24) >> 1, lane_word, e[3], o[3], p.one);
+      accumulate_entries<0>(smem_words, rec, pos, counts & 0xffu, lane_word, e[0], o[0], p.one);
+      accumulate_entries<1>(smem_words, rec, pos, (counts >> 8) & 0xffu, lane_word, e[1], o[1], p.one);
+      accumulate_entries<2>(smem_words, rec, pos, (counts >> 16) & 0xffu, lane_word, e[2], o[2], p.one);
+      accumulate_entries<3>(smem_words, rec, pos, counts >> 24, lane_word, e[3], o[3], p.one);
       if ((k + 1) % chunks_per_flush == 0 || k + 1 == p.nchunks) {
         flush_class<0>(e[0], o[0], acc, lane);
         flush_class<1>(e[1], o[1], acc, lane);
@@ -262,7 +379,32 @@ __device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int
         flush_class<3>(e[3], o[3], acc, lane);
       }
     }
-    __syncthreads();  // buffer k & 1 is restaged for chunk k + 2
+    // release the stage; the last warp out refills it with chunk k + stages
+    __syncwarp();
+    uint32_t last = 0;
+    if (lane == 0) {
+      last = release_stage(&ps.released[s]) == static_cast<uint32_t>(kWarps - 1) ? 1u : 0u;
+      if (last) ps.released[s] = 0;
+    }
+    last = __shfl_sync(kFull, last, 0);
+    if (last && k + p.stages < p.nchunks)
+      issue_chunk(p, ps, smem, k + p.stages, s, group, block, t0, dm_limit, group_rows);
+    if (++s == p.stages) {
+      s = 0;
+      parity ^= 1u;
+    }
+  }
+  if (!ok) {
+    // give up: flag it, let the copies already issued to this stage land
+    // (bounded), and write nothing
+    if (lane == 0) {
+      *reinterpret_cast<volatile uint32_t*>(&ps.failed) = 1u;
+      atomicOr(p.status, GF_STATUS_PIPELINE);
+    }
+    const long long start = clock64();
+    while (!mbar_try_wait(&ps.full[s], parity) && clock64() - start < kWaitCycles) {
+    }
+    return;
   }
   if (!active) return;
   OutT* out = static_cast<OutT*>(p.out) +
@@ -289,8 +431,9 @@ __device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int
 
 template <typename OutT>
 __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesParams p) {
-  extern __shared__ __align__(16) uint8_t smem[];
-  bytes_cta<OutT>(p, blockIdx.x, static_cast<int>(blockIdx.z), smem);
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ PipeShared ps;
+  bytes_cta<OutT>(p, blockIdx.x, static_cast<int>(blockIdx.z), smem, ps);
 }
 
 // Many launches (programs, DM ranges, observations) as one grid: CTA b runs
@@ -298,9 +441,10 @@ __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_kernel(BytesPara
 __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_batch_kernel(const BytesParams* __restrict__ items,
                                                                              const uint64_t* __restrict__ block_begin,
                                                                              int nitems) {
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   __shared__ BytesParams sp;
   __shared__ uint32_t s_local;
+  __shared__ PipeShared ps;
   if (threadIdx.x == 0) {
     const uint64_t b = blockIdx.x;
     int lo = 0, hi = nitems;
@@ -313,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, 2) dedisperse_bytes_batch_kernel(con
   }
   __syncthreads();
   const uint32_t local = s_local;
-  bytes_cta<uint32_t>(sp, local % sp.grid_x, static_cast<int>(local / sp.grid_x), smem);
+  bytes_cta<uint32_t>(sp, local % sp.grid_x, static_cast<int>(local / sp.grid_x), smem, ps);
 }
 
 // Stage-2 sum over uint32 intermediate rows (subband with 8-bit input, where
@@ -392,8 +536,9 @@ __global__ void __launch_bounds__(256) stage_kernel(const uint8_t* __restrict__ 
   }
 }
 
-// Class-sorted gather records: word 0 packs the four (even) class counts,
-// then (chunk_rows + 4) / 2 words of u16 entry pairs.
+// Class-sorted gather records: word 0 packs the four class counts (channels
+// of byte class 0..3), then (chunk_rows + 4) / 2 words of u16 entry pairs
+// (word offsets into the stage: row * row_bytes / 4 + delay offset / 4).
 struct Records {
   std::vector<uint32_t> words;
   std::vector<int32_t> base;
@@ -413,7 +558,6 @@ Records build_records(const std::vector<int32_t>& delays, int ngroups, int ndm_g
   r.record_words = static_cast<int>(round_up(1 + (chunk_rows + 4) / 2, 4));
   r.base.assign(static_cast<size_t>(ngroups) * blocks * rows_per_group, 0);
   r.words.assign(static_cast<size_t>(ngroups) * ndm_group * r.nchunks * r.record_words, 0u);
-  const int zero_word = chunk_rows * row_bytes / 4;
   std::vector<uint16_t> cls[4];
   for (int g = 0; g < ngroups; ++g) {
     const int grows = std::min(rows_per_group, total_rows - g * rows_per_group);
@@ -443,8 +587,10 @@ Records build_records(const std::vector<int32_t>& delays, int ngroups, int ndm_g
         uint32_t counts = 0;
         std::vector<uint16_t> flat;
         for (int s = 0; s < 4; ++s) {
-          if (cls[s].size() & 1) cls[s].push_back(static_cast<uint16_t>(zero_word));
+          // the count is the class's channels; an odd class takes a whole
+          // word for its last entry (high half unused), so classes start on words
           counts |= static_cast<uint32_t>(cls[s].size()) << (8 * s);
+          if (cls[s].size() & 1) cls[s].push_back(0);
           flat.insert(flat.end(), cls[s].begin(), cls[s].end());
         }
         rec[0] = counts;
@@ -461,16 +607,20 @@ struct Launch {
   int warps_per_dm = 1;
   int chunk_rows = 64;
   int row_bytes = 0;
+  int stages = 2;
+  uint32_t stage_bytes = 0;
   size_t smem = 0;
 };
 
-// Picks the DM block size and channel chunk so the staged windows fit in
-// shared memory with two CTAs per SM when possible.
-// dpc_fix / cr_fix (0 = any) pin the DM block or the chunk rows (launch
-// shapes picked by an autotuner); every shape gives the same sums.
+// Picks the DM block size, channel chunk and ring depth so the stages fit in
+// shared memory with two CTAs per SM when possible (228 KB per SM, 1 KB
+// reserved per CTA, the ring state and batch table in static shared memory):
+// the largest chunk with 3 stages, else with 2.  dpc_fix / cr_fix (0 = any)
+// pin the DM block or the chunk rows (launch shapes picked by an autotuner);
+// every shape gives the same sums.
 template <typename F>
 Launch choose_launch(F&& max_off_for, int dpc_fix, int cr_fix) {
-  const size_t budget2 = 110 * 1024, budget1 = 220 * 1024;
+  const size_t budget2 = 112 * 1024, budget1 = 224 * 1024;
   for (size_t budget : {budget2, budget1}) {
     for (int dpc : {8, 4, 2, 1}) {
       if (dpc_fix && dpc != dpc_fix) continue;
@@ -480,9 +630,11 @@ Launch choose_launch(F&& max_off_for, int dpc_fix, int cr_fix) {
       for (int cr : {64, 32, 16, 8}) {
         if (cr_fix && cr != cr_fix) continue;
         const size_t rec = static_cast<size_t>(dpc) * round_up(1 + (cr + 4) / 2, 4) * 4;
-        const size_t smem = 2 * (static_cast<size_t>(cr + 1) * row_bytes + rec);  // double-buffered
-        if (smem <= budget && static_cast<size_t>(cr + 1) * row_bytes < 262144) {
-          return Launch{dpc, wpd, cr, row_bytes, smem};
+        const size_t stage = static_cast<size_t>(cr) * row_bytes + rec;
+        if (static_cast<size_t>(cr) * row_bytes >= 65536 * 4) continue;  // u16 word offsets
+        for (int st : {3, 2}) {
+          if (st * stage <= budget)
+            return Launch{dpc, wpd, cr, row_bytes, st, static_cast<uint32_t>(stage), st * stage};
         }
       }
     }
@@ -512,7 +664,7 @@ int max_off_estimate(const std::vector<int32_t>& delays, int ngroups, int ndm_gr
 struct BytesStage {
   Launch launch;
   Records rec;
-  DeviceBlob base_dev, rec_dev;
+  DeviceBlob base_dev, rec_dev, status_dev;
   int ngroups = 0, ndm_group = 0, rows_per_group = 0, total_rows = 0, blocks = 0;
 
   void build(const std::vector<int32_t>& delays, int ng, int ndg, int rpg, int tr, int device, int dpc_fix = 0,
@@ -527,6 +679,18 @@ struct BytesStage {
     rec = build_records(delays, ng, ndg, rpg, tr, launch.dms_per_cta, launch.chunk_rows, launch.row_bytes);
     base_dev.upload(rec.base.data(), rec.base.size() * sizeof(int32_t), device);
     rec_dev.upload(rec.words.data(), rec.words.size() * sizeof(uint32_t), device);
+    const uint32_t zero = 0;
+    status_dev.upload(&zero, sizeof zero, device);
+  }
+
+  // Reads and clears the status word (GF_STATUS_PIPELINE: a launch gave up).
+  uint32_t take_status(cudaStream_t stream) const {
+    if (!status_dev.ptr) return 0;
+    uint32_t v = 0;
+    cuda_check(cudaMemcpyAsync(&v, status_dev.ptr, sizeof v, cudaMemcpyDeviceToHost, stream), "dedispersion status");
+    cuda_check(cudaStreamSynchronize(stream), "dedispersion status");
+    if (v) cuda_check(cudaMemsetAsync(status_dev.ptr, 0, sizeof v, stream), "dedispersion status reset");
+    return v;
   }
 
   uint64_t metadata_bytes() const { return base_dev.bytes + rec_dev.bytes; }
@@ -540,6 +704,10 @@ struct BytesStage {
                      uint64_t out_row_stride, uint64_t out_dm_rows, uint64_t out_group_rows,
                      uint64_t nout) const {
     if (dm_first % launch.dms_per_cta != 0) raise(GF_EINVAL, "DM range not aligned to the DM block");
+    // bulk copies: 16-byte aligned rows
+    check_arg(reinterpret_cast<uintptr_t>(in) % 16 == 0 && row_stride % 16 == 0 && group_stride % 16 == 0,
+              "dedispersion input must be 16-byte aligned");
+    check_arg(valid <= row_stride, "dedispersion row stride below the valid samples");
     BytesParams p{};
     p.in = in;
     p.in_row_stride = row_stride;
@@ -574,6 +742,9 @@ struct BytesStage {
     const uint64_t ctas = ceil_div(nout, p.cta_samples) * static_cast<uint64_t>(p.nblocks);
     if (ctas >= (1ull << 31)) raise(GF_EINVAL, "dedispersion launch too large");
     p.grid_x = static_cast<uint32_t>(ctas);
+    p.stages = launch.stages;
+    p.stage_bytes = launch.stage_bytes;
+    p.status = status_dev.as<uint32_t>();
     return p;
   }
 
@@ -878,6 +1049,17 @@ extern "C" int gf_dedisp_run(gf_dedisp_program* P, const void* dev_staged, uint6
       }
       cuda_check(cudaGetLastError(), "subband stage 2 launch");
     }
+  });
+}
+
+extern "C" int gf_dedisp_check(gf_dedisp_program* P, void* stream) {
+  return guarded([&] {
+    check_arg(P != nullptr, "null argument");
+    DeviceGuard dg(P->desc.device_id);
+    auto s = as_stream(stream);
+    const uint32_t v = P->brute.take_status(s) | P->stage1.take_status(s) | P->stage2.take_status(s);
+    if (v & GF_STATUS_PIPELINE)
+      raise(GF_ERUNTIME, "dedispersion: a shared-memory copy stage did not complete (internal error)");
   });
 }
 

@@ -295,6 +295,7 @@ def _dedisperse(filterbank: Filterbank, dm_low: float, dm_step: float, ndm: int,
     with torch.cuda.device(dev):
         staged = prog.stage(torch.from_numpy(np.ascontiguousarray(samples)).to(f"cuda:{dev}"))
         out = prog.run(staged, 0, int(ndm))
+        prog.check()
         host = out[:, : prog.nout].contiguous().cpu().numpy().view(np.uint32)
     return DedispersedResult(np.ascontiguousarray(host), tsamp=tsamp, dm_low=dm_low,
                              dm_step=dm_step if ndm > 1 or algorithm == "subband" else 0.0, backend="cuda")

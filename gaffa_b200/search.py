@@ -169,6 +169,7 @@ class DmSearch:
                 parts.append(self.ffa.expand(rec, b0, self.dm_low, self.dm_step))
             launches += dd_kernels + 4 + 1 + ffa_kernels
         self.pre.synchronize()
+        self.dedisp.check()
         if self.device_candidates:
             return parts, launches
         peaks = np.concatenate(parts) if parts else np.zeros(0, _lib.PEAK_DTYPE)
@@ -196,6 +197,7 @@ class DmSearch:
         if self.dedisp.algorithm == "subband":
             ws = torch.empty(self.dedisp.workspace_bytes(cnt), dtype=torch.uint8, device=self.device)
         dd = self.dedisp.run(staged, b0, cnt, out_stride=self.out_stride, workspace=ws)
+        self.dedisp.check()
         row = dd[dm_index - b0, : self.nout]
         return core.fold_time_series(row, period, self.tsamp, self.fold_nbin)
 

@@ -39,6 +39,7 @@ extern "C" {
 #define GF_STATUS_CONSTANT 2u
 #define GF_STATUS_PEAK_OVERFLOW 4u
 #define GF_STATUS_SCHEDULE 8u /* an FFA block schedule exceeded its tile (internal error) */
+#define GF_STATUS_PIPELINE 16u /* a dedispersion copy stage did not complete within ~2 s (internal error) */
 
 const char* gf_last_error(void);
 const char* gf_status_string(int status);
@@ -163,7 +164,9 @@ int gf_dedisp_stage_from_host(gf_dedisp_program* program, const void* host_input
  * dedisperse_multi_dm_cpu (dedispersion.cpp:291-329) or
  * dedisperse_subband_cpu (:331-453).  Replaces multi_dm_kernel and
  * subband_stage1/2_kernel, dedispersion_cuda.cu:320-417.  Subband runs need
- * dm_begin / dm_count aligned to ndm_per_nominal (except at the end). */
+ * dm_begin / dm_count aligned to ndm_per_nominal (except at the end).
+ * dev_staged and dev_workspace must be 16-byte aligned (the kernels copy
+ * their rows with bulk copies); cudaMalloc'd buffers are. */
 int gf_dedisp_run(gf_dedisp_program* program, const void* dev_staged,
                   uint64_t dm_begin, uint64_t dm_count, uint32_t* dev_out,
                   uint64_t out_stride, void* dev_workspace, void* stream);
@@ -186,6 +189,14 @@ int gf_dedisp_batch_create(const gf_dedisp_batch_item* items, uint64_t nitems,
                            gf_dedisp_batch** out);
 int gf_dedisp_batch_run(gf_dedisp_batch* batch, void* stream);
 int gf_dedisp_batch_destroy(gf_dedisp_batch* batch);
+
+/* Synchronises `stream` and reads (and clears) the program's device status
+ * word: GF_ERUNTIME when a launch of gf_dedisp_run or gf_dedisp_batch_run gave
+ * up waiting for one of its shared-memory copy stages (every wait is bounded;
+ * such a launch writes no output).  Call after a group of runs, before their
+ * output is used.  No reference counterpart: the reference's kernels have no
+ * waits (dedispersion_cuda.cu:320-417). */
+int gf_dedisp_check(gf_dedisp_program* program, void* stream);
 
 /* Workspace bytes gf_dedisp_run needs for a batch of dm_count DMs (0 for
  * brute force; the subband intermediate otherwise).  Brute-force batches start
