@@ -83,6 +83,11 @@ class FfaMemberInfo(C.Structure):
                 ("ntasks", u64), ("noctaves", u64)]
 
 
+class PreprocessBatchItem(C.Structure):
+    _fields_ = [("desc", C.POINTER(PreprocessDesc)), ("dev_series", vp), ("input_is_u32", i32), ("reserved", i32),
+                ("nseries", u64), ("stride", u64), ("dev_workspace", vp), ("dev_stats", vp), ("dev_status", vp)]
+
+
 class DedispBatchItem(C.Structure):
     _fields_ = [("program", vp), ("dev_staged", vp), ("dm_begin", u64), ("dm_count", u64), ("dev_out", vp),
                 ("out_stride", u64)]
@@ -180,6 +185,9 @@ _SIGNATURES = [
     ("gf_preprocess_info_get", C.c_int, [C.POINTER(PreprocessDesc), C.POINTER(PreprocessInfo)]),
     ("gf_preprocess_inplace", C.c_int, [C.POINTER(PreprocessDesc), vp, i32, u64, u64, vp, vp, vp, vp]),
     ("gf_normalise", C.c_int, [vp, u64, u64, u64, vp, vp]),
+    ("gf_preprocess_batch_create", C.c_int, [C.POINTER(PreprocessBatchItem), u64, i32, C.POINTER(vp)]),
+    ("gf_preprocess_batch_run", C.c_int, [vp, vp]),
+    ("gf_preprocess_batch_destroy", C.c_int, [vp]),
     ("gf_ffa_program_create", C.c_int, [vp, u64, vp, u64, u64, i32, C.POINTER(vp)]),
     ("gf_ffa_program_destroy", C.c_int, [vp]),
     ("gf_ffa_program_info", C.c_int, [vp, C.POINTER(FfaInfo)]),
@@ -194,6 +202,8 @@ _SIGNATURES = [
     ("gf_ffa_batch_member_info", C.c_int, [vp, u64, C.POINTER(FfaMemberInfo)]),
     ("gf_ffa_batch_bind", C.c_int, [vp, C.POINTER(vp)]),
     ("gf_ffa_batch_prepare", C.c_int, [vp, u64, vp, u64, vp, vp]),
+    ("gf_ffa_batch_bind_series", C.c_int, [vp, C.POINTER(vp), C.POINTER(u64), C.POINTER(vp)]),
+    ("gf_ffa_batch_prepare_all", C.c_int, [vp, vp]),
     ("gf_ffa_batch_search", C.c_int, [vp, C.c_float, vp, vp, u64, vp, vp]),
     ("gf_ffa_batch_expand_peaks", C.c_int, [vp, vp, u64, vp, vp, vp, vp, vp]),
     ("gf_sort_peaks", C.c_int, [vp, u64]),

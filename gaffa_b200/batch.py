@@ -10,8 +10,10 @@ the pieces are packed into waves that fit the series arena.  Each wave runs
 
 * ONE dedispersion launch over all its pieces (gf_dedisp_batch: each CTA
   finds its piece in a block table),
-* per piece, the detrend/normalise and FFA-prepare kernels of its
-  observation (the prepare folds every octave's downsampling into one pass),
+* ONE launch per preprocessing stage (scrunch, running median, detrend,
+  statistics) and ONE FFA-prepare launch over all its pieces
+  (gf_preprocess_batch, gf_ffa_batch_prepare_all: item tables likewise; the
+  prepare folds every octave's downsampling into one pass),
 * ONE persistent FFA launch per class over every (piece series, task) item
   of the wave (gf_ffa_batch: the item runs of all members in one table),
 
@@ -138,6 +140,7 @@ class _Wave:
         self.pieces = pieces
         self.series = []
         self.dd = None
+        self.pre = None
         self.ffa = None
         self.graph = None
 
@@ -233,6 +236,10 @@ class BatchSearch:
                 for pc, s in zip(w.pieces, series))
             w.ffa = core.FfaBatchProgram([(self.plans[pc.obs], pc.dm_count) for pc in w.pieces],
                                          device_id=self.device_id, prepared=prepared, scratch=False)
+            # one launch per preprocessing stage and one prepare over every piece
+            w.pre = core.PreprocessBatch((self.pre[pc.obs], sr, pc.dm_count) for pc, sr in zip(w.pieces, series))
+            w.ffa.bind_series([sr.view(torch.float32) for sr in series],
+                              [self.pre[pc.obs].stats[: pc.dm_count] for pc in w.pieces])
             w.graph = None
         need = max(w.ffa.scratch_bytes for w in self.waves)
         self._scratch = torch.empty(max(16, need), dtype=torch.uint8, device=self.device)
@@ -244,9 +251,8 @@ class BatchSearch:
 
     def _launch_wave(self, w: _Wave) -> None:
         w.dd.run()
-        for m, pc in enumerate(w.pieces):
-            stats = self.pre[pc.obs].run(w.series[m], pc.dm_count)
-            w.ffa.prepare(m, w.series[m].view(torch.float32), stats)
+        w.pre.run()
+        w.ffa.prepare_all()
         w.ffa.search_async(self.snr_threshold)
 
     def _run_wave(self, w: _Wave) -> None:
@@ -271,10 +277,13 @@ class BatchSearch:
 
     @property
     def kernel_launches_per_run(self) -> int:
-        """Kernels one run launches in its waves (one dedispersion launch,
-        four detrend/normalise kernels and one prepare per piece, the FFA
-        classes); each observation's fold adds three."""
-        return sum(1 + w.ffa.kernel_launches + 5 * len(w.pieces) for w in self.waves)
+        """Kernels one run launches in its waves: per wave one dedispersion
+        launch, three or four preprocessing stages (scrunch, running median,
+        detrend, statistics) and one prepare over all its pieces, and one
+        FFA launch per class; each observation's fold adds three."""
+        if not self._built:
+            raise RuntimeError("the waves are built by the first run()")
+        return sum(1 + w.pre.kernel_launches + 1 + w.ffa.kernel_launches for w in self.waves)
 
     def stage(self, filterbanks) -> None:
         """Stages every observation's time-major filterbank (device tensor or

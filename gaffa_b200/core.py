@@ -314,6 +314,60 @@ class PreprocessProgram:
                                           ptr(self.stats), _stream(stream)))
 
 
+class PreprocessBatch:
+    """Many PreprocessProgram.run calls (series sets of different lengths and
+    windows) as one launch per stage (gf_preprocess_batch_*).  items:
+    [(PreprocessProgram, series [nseries][stride] int32 or float32, nseries)];
+    each program's statistics and status receive its item's results, as
+    run() would.  Pointers are fixed here, so run() can be captured in a CUDA
+    graph; the tensors must stay alive as long as the batch."""
+
+    def __init__(self, items):
+        items = list(items)
+        if not items:
+            raise ValueError("batched preprocessing needs at least one item")
+        arr = (_lib.PreprocessBatchItem * len(items))()
+        self._keep = []
+        device = None
+        for i, (pre, series, nseries) in enumerate(items):
+            if series.dim() != 2:
+                raise ValueError("series must be [nseries][stride]")
+            is_u32 = series.dtype in (torch.int32, torch.uint32)
+            if not is_u32 and series.dtype != torch.float32:
+                raise TypeError("series must be uint32 (int32 storage) or float32")
+            arr[i].desc = C.pointer(pre.desc)
+            arr[i].dev_series = ptr(series)
+            arr[i].input_is_u32 = int(is_u32)
+            arr[i].nseries, arr[i].stride = int(nseries), series.stride(0)
+            arr[i].dev_workspace, arr[i].dev_stats, arr[i].dev_status = ptr(pre.workspace), ptr(pre.stats), \
+                ptr(pre.status)
+            self._keep += [pre, series]
+            if device is not None and pre.device != device:
+                raise ValueError("batched preprocessing items must share one device")
+            device = pre.device
+        self.device = device
+        h = C.c_void_p()
+        with torch.cuda.device(device):
+            check(_lib.lib().gf_preprocess_batch_create(arr, len(items), device.index or 0, C.byref(h)))
+        self._h = h
+        self.scrunched = any(int(p.info.scrunch_factor) > 1 for p, _, _ in items)
+
+    @property
+    def kernel_launches(self) -> int:
+        return 4 if self.scrunched else 3
+
+    def run(self, stream=None) -> None:
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_preprocess_batch_run(self._h, _stream(stream)))
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.gf_preprocess_batch_destroy(h)
+
+    __del__ = close
+
+
 # ---------------------------------------------------------------------------
 # FFA
 # ---------------------------------------------------------------------------
@@ -507,6 +561,28 @@ class FfaBatchProgram:
         with torch.cuda.device(self.device):
             check(_lib.lib().gf_ffa_batch_prepare(self._h, member, ptr(series), series.stride(0), ptr(stats),
                                                   _stream(stream)))
+
+    def bind_series(self, series, stats) -> None:
+        """The inputs prepare_all reads: per member a float32 [nseries][stride]
+        series view and its FP64 [nseries][2] statistics (None: no
+        normalisation).  Pointers are fixed here (capturable launches)."""
+        n = len(self.prepared)
+        if len(series) != n or len(stats) != n:
+            raise ValueError("one series view and one statistics table per member")
+        for t in series:
+            if t.dtype != torch.float32 or t.dim() != 2:
+                raise TypeError("series views must be float32 [nseries][stride]")
+        sp = (C.c_void_p * n)(*[t.data_ptr() for t in series])
+        st = (_lib.u64 * n)(*[t.stride(0) for t in series])
+        ss = (C.c_void_p * n)(*[(t.data_ptr() if t is not None else None) for t in stats])
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_ffa_batch_bind_series(self._h, sp, st, ss))
+        self._bound_series = (list(series), list(stats))
+
+    def prepare_all(self, stream=None) -> None:
+        """prepare() of every member, in one launch (after bind_series)."""
+        with torch.cuda.device(self.device):
+            check(_lib.lib().gf_ffa_batch_prepare_all(self._h, _stream(stream)))
 
     def search_async(self, snr_threshold: float, stream=None) -> None:
         if self.scratch is None:

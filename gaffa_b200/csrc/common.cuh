@@ -62,8 +62,8 @@ inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 __host__ __device__ inline uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 __host__ __device__ inline uint32_t umin32(uint32_t a, uint32_t b) { return a < b ? a : b; }
 
-inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
-inline uint64_t round_up(uint64_t a, uint64_t b) { return ceil_div(a, b) * b; }
+__host__ __device__ inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline uint64_t round_up(uint64_t a, uint64_t b) { return ceil_div(a, b) * b; }
 
 // Sets the current device for the scope and restores the caller's device.
 struct DeviceGuard {

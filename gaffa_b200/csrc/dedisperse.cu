@@ -75,8 +75,9 @@ struct BytesParams {
   uint64_t in_valid;         // valid samples per row (zero beyond)
   int rows_per_group;
   int total_rows;            // group g has min(rows_per_group, total_rows - g*rows_per_group) rows
-  const int32_t* base;       // + g*base_group_stride + dm_block*rows_per_group
+  const int32_t* base;       // + g*base_group_stride + dm_block*base_block_stride
   uint64_t base_group_stride;
+  uint64_t base_block_stride; // rows_per_group rounded up to 4 (16-byte aligned chunk rows)
   const uint32_t* records;   // + g*rec_group_stride + dm*rec_dm_stride + chunk*record_words
   uint64_t rec_group_stride;
   uint64_t rec_dm_stride;
@@ -99,7 +100,8 @@ struct BytesParams {
   uint64_t nout;             // valid output samples
   uint32_t grid_x;           // CTAs per group (grid x)
   int stages;                // shared-memory stages in the copy ring (2-4)
-  uint32_t stage_bytes;      // chunk_rows * row_bytes + dms_per_cta * record_words * 4
+  uint32_t stage_bytes;      // windows, records and the window bases of the chunk `stages` ahead
+  uint32_t base_bytes;       // chunk_rows * 4 rounded up to 16
   uint32_t* status;          // GF_STATUS_PIPELINE when a stage wait gives up
 };
 
@@ -117,14 +119,15 @@ __device__ __forceinline__ uint32_t pos_sum(uint32_t e, uint32_t o, int b) {
   return b == 0 ? lo16(e) : b == 1 ? lo16(o) : b == 2 ? hi16(e) : hi16(o);
 }
 
+// acc: the warp's 32-bit sums in shared memory, [m][position][lane].
 template <int S>
-__device__ __forceinline__ void flush_class(uint32_t (&e)[kWords], uint32_t (&o)[kWords],
-                                            uint32_t (&out)[kWords][4], int lane) {
+__device__ __forceinline__ void flush_class(uint32_t (&e)[kWords], uint32_t (&o)[kWords], uint32_t* acc,
+                                            int lane) {
 #pragma unroll
   for (int m = 0; m < kWords; ++m) {
     if (S == 0) {
 #pragma unroll
-      for (int p = 0; p < 4; ++p) out[m][p] += pos_sum(e[m], o[m], p);
+      for (int p = 0; p < 4; ++p) acc[(m * 4 + p) * 32 + lane] += pos_sum(e[m], o[m], p);
     } else {
       // class S word j contributes to output positions p = b - S of word j
       // (b >= S) and p = b - S + 4 of word j - 1 (b < S); so output word j
@@ -137,7 +140,7 @@ __device__ __forceinline__ void flush_class(uint32_t (&e)[kWords], uint32_t (&o)
 #pragma unroll
       for (int p = 0; p < 4; ++p) {
         const int b = p + S;
-        out[m][p] += b < 4 ? pos_sum(e[m], o[m], b) : pos_sum(ne, no, b - 4);
+        acc[(m * 4 + p) * 32 + lane] += b < 4 ? pos_sum(e[m], o[m], b) : pos_sum(ne, no, b - 4);
       }
     }
     e[m] = 0u;
@@ -150,8 +153,10 @@ __device__ __forceinline__ void accumulate_class(const uint32_t* __restrict__ sm
                                                  const uint32_t* __restrict__ rec, int& pos,
                                                  int npairs, int lane_word,
                                                  uint32_t (&e)[kWords], uint32_t (&o)[kWords], uint32_t one) {
+  uint32_t next = npairs > 0 ? rec[pos] : 0u;  // the next pair's entry loads a pair ahead
   for (int i = 0; i < npairs; ++i) {
-    const uint32_t entry = rec[pos + i];
+    const uint32_t entry = next;
+    next = rec[pos + i + 1];
     const uint32_t* a = smem_words + (entry & 0xffffu) + lane_word;
     const uint32_t* b = smem_words + (entry >> 16) + lane_word;
 #pragma unroll
@@ -256,34 +261,41 @@ __device__ __forceinline__ bool wait_stage(uint64_t* bar, uint32_t parity, const
 // The calling warp stages chunk k of CTA (group, block, t0) into stage s:
 // lane r copies channel rows r and r + 32 (bulk below the last 16-byte
 // boundary of the valid samples, by hand with zeros past them), lanes
-// d < dms_per_cta the records of DM d.  The stage's barrier completes after
-// the 32 lane arrivals and the bytes that lane 0 announced.  Runs once per
-// chunk; rows are taken one at a time (row windows recomputed in the second
-// pass) to keep its registers few next to the summing loop's accumulators.
+// d < dms_per_cta the records of DM d, and one lane the window bases of chunk
+// k + stages (read by the warp that refills this stage).  The window bases of
+// chunk k come from `bases` (shared memory; global for the first chunks).
+// The stage's barrier completes after the 32 lane arrivals and the bytes
+// that lane 0 announced.  Rows are taken one at a time to keep this path's
+// registers few next to the summing loop's accumulators.
 __device__ __forceinline__ uint32_t row_bulk_bytes(const BytesParams& p, uint64_t t_row) {
   const uint64_t bulk_end = p.in_valid & ~15ull;
   return t_row < bulk_end ? static_cast<uint32_t>(umin64(p.row_bytes, bulk_end - t_row)) : 0u;
 }
 
 __device__ __forceinline__ void issue_chunk(const BytesParams& p, PipeShared& ps, uint8_t* smem, int k, int s,
-                                            int group, int block, uint64_t t0, int dm_limit, int group_rows) {
+                                            int group, int block, uint64_t t0, int dm_limit, int group_rows,
+                                            const int32_t* bases) {
   const int lane = threadIdx.x & 31;
-  const int32_t* base = p.base + group * p.base_group_stride + static_cast<uint64_t>(block) * p.rows_per_group;
+  const int32_t* gbase = p.base + group * p.base_group_stride + static_cast<uint64_t>(block) * p.base_block_stride;
   const int row0 = k * p.chunk_rows;
   const int nrows = min(p.chunk_rows, group_rows - row0);
   const int dl = block * p.dms_per_cta + lane;
   const bool rec_copy = lane < p.dms_per_cta && dl < dm_limit;
+  const bool base_copy = lane == 31 && k + p.stages < p.nchunks;
   uint32_t bytes = rec_copy ? static_cast<uint32_t>(p.record_words) * 4u : 0u;
+  if (base_copy) bytes += p.base_bytes;
 #pragma unroll 1
-  for (int r = lane; r < nrows; r += 32) bytes += row_bulk_bytes(p, t0 + static_cast<uint64_t>(base[row0 + r]));
+  for (int r = lane; r < nrows; r += 32) bytes += row_bulk_bytes(p, t0 + static_cast<uint64_t>(bases[r]));
   const uint32_t total = __reduce_add_sync(kFull, bytes);
   if (lane == 0) mbar_expect_tx(&ps.full[s], total);
   __syncwarp();
-  fence_proxy_async_smem();  // earlier generic accesses of the stage before the copies' writes
+  fence_proxy_async_smem();  // earlier accesses of the stage before the copies' writes
   uint8_t* rows = smem + static_cast<uint32_t>(s) * p.stage_bytes;
+  const uint32_t rows_bytes = static_cast<uint32_t>(p.chunk_rows) * p.row_bytes;
+  const uint32_t rec_bytes = static_cast<uint32_t>(p.dms_per_cta * p.record_words) * 4u;
 #pragma unroll 1
   for (int r = lane; r < nrows; r += 32) {
-    const uint64_t t_row = t0 + static_cast<uint64_t>(base[row0 + r]);
+    const uint64_t t_row = t0 + static_cast<uint64_t>(bases[r]);
     const uint32_t nbulk = row_bulk_bytes(p, t_row);
     const uint8_t* src = p.in + group * p.in_group_stride + static_cast<uint64_t>(row0 + r) * p.in_row_stride;
     uint8_t* dst = rows + r * p.row_bytes;
@@ -302,11 +314,17 @@ __device__ __forceinline__ void issue_chunk(const BytesParams& p, PipeShared& ps
     }
   }
   if (rec_copy)
-    bulk_copy(reinterpret_cast<uint32_t*>(rows + static_cast<uint32_t>(p.chunk_rows) * p.row_bytes) +
-                  lane * p.record_words,
+    bulk_copy(reinterpret_cast<uint32_t*>(rows + rows_bytes) + lane * p.record_words,
               p.records + group * p.rec_group_stride + dl * p.rec_dm_stride +
                   static_cast<uint64_t>(k) * p.record_words,
               static_cast<uint32_t>(p.record_words) * 4u, &ps.full[s]);
+  // every lane has read `bases` (which may be this stage's base area) before
+  // the copy of the next bases overwrites it
+  __syncwarp();
+  fence_proxy_async_smem();
+  if (base_copy)
+    bulk_copy(rows + rows_bytes + rec_bytes, gbase + static_cast<uint64_t>(k + p.stages) * p.chunk_rows,
+              p.base_bytes, &ps.full[s]);
   mbar_arrive(&ps.full[s]);
 }
 
@@ -341,19 +359,27 @@ __device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int
   __syncthreads();
   if (ps.failed) return;
 
-  uint32_t e[4][kWords], o[4][kWords], acc[kWords][4];
+  // 16-bit lane sums per byte class in registers; 32-bit sums in shared
+  // memory after the ring ([warp][m][position][lane], conflict-free)
+  uint32_t e[4][kWords], o[4][kWords];
+  uint32_t* acc = reinterpret_cast<uint32_t*>(smem + static_cast<uint32_t>(p.stages) * p.stage_bytes) +
+                  warp * (kWords * 4 * 32);
 #pragma unroll
   for (int m = 0; m < kWords; ++m) {
 #pragma unroll
     for (int s = 0; s < 4; ++s) { e[s][m] = 0u; o[s][m] = 0u; }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[m][q] = 0u;
+    for (int q = 0; q < 4; ++q) acc[(m * 4 + q) * 32 + lane] = 0u;
   }
   const int lane_word = sub * kOutWords + lane;
   const int chunks_per_flush = kFlushChannels / p.chunk_rows;
 
-  if (warp == 0)
-    for (int k = 0; k < min(p.stages, p.nchunks); ++k) issue_chunk(p, ps, smem, k, k, group, block, t0, dm_limit, group_rows);
+  if (warp == 0) {
+    const int32_t* gbase =
+        p.base + group * p.base_group_stride + static_cast<uint64_t>(block) * p.base_block_stride;
+    for (int k = 0; k < min(p.stages, p.nchunks); ++k)
+      issue_chunk(p, ps, smem, k, k, group, block, t0, dm_limit, group_rows, gbase + k * p.chunk_rows);
+  }
   int s = 0;
   uint32_t parity = 0;
   bool ok = true;
@@ -387,8 +413,13 @@ __device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int
       if (last) ps.released[s] = 0;
     }
     last = __shfl_sync(kFull, last, 0);
-    if (last && k + p.stages < p.nchunks)
-      issue_chunk(p, ps, smem, k + p.stages, s, group, block, t0, dm_limit, group_rows);
+    if (last && k + p.stages < p.nchunks) {
+      const uint8_t* stage = smem + static_cast<uint32_t>(s) * p.stage_bytes;
+      const int32_t* next_bases = reinterpret_cast<const int32_t*>(
+          stage + static_cast<uint32_t>(p.chunk_rows) * p.row_bytes +
+          static_cast<uint32_t>(p.dms_per_cta * p.record_words) * 4u);
+      issue_chunk(p, ps, smem, k + p.stages, s, group, block, t0, dm_limit, group_rows, next_bases);
+    }
     if (++s == p.stages) {
       s = 0;
       parity ^= 1u;
@@ -417,14 +448,17 @@ __device__ __forceinline__ void bytes_cta(const BytesParams& p, unsigned bx, int
     const uint64_t t = t0 + static_cast<uint64_t>(sub) * kWarpSamples + 4ull * j;
     if (t >= p.nout) continue;
     if (sizeof(OutT) == 4 && t + 4 <= p.nout && (p.out_row_stride & 3) == 0) {
-      *reinterpret_cast<uint4*>(out + t) = make_uint4(acc[m][0], acc[m][1], acc[m][2], acc[m][3]);
+      *reinterpret_cast<uint4*>(out + t) =
+          make_uint4(acc[(m * 4) * 32 + lane], acc[(m * 4 + 1) * 32 + lane], acc[(m * 4 + 2) * 32 + lane],
+                     acc[(m * 4 + 3) * 32 + lane]);
     } else if (sizeof(OutT) == 1 && t + 4 <= p.nout && (p.out_row_stride & 3) == 0) {
       *reinterpret_cast<uint32_t*>(out + t) =
-          acc[m][0] | (acc[m][1] << 8) | (acc[m][2] << 16) | (acc[m][3] << 24);
+          acc[(m * 4) * 32 + lane] | (acc[(m * 4 + 1) * 32 + lane] << 8) | (acc[(m * 4 + 2) * 32 + lane] << 16) |
+          (acc[(m * 4 + 3) * 32 + lane] << 24);
     } else {
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (t + q < p.nout) out[t + q] = static_cast<OutT>(acc[m][q]);
+        if (t + q < p.nout) out[t + q] = static_cast<OutT>(acc[(m * 4 + q) * 32 + lane]);
     }
   }
 }
@@ -541,14 +575,16 @@ __global__ void __launch_bounds__(256) stage_kernel(const uint8_t* __restrict__ 
 // (word offsets into the stage: row * row_bytes / 4 + delay offset / 4).
 struct Records {
   std::vector<uint32_t> words;
-  std::vector<int32_t> base;
+  std::vector<int32_t> base;  // [group][block][base_stride]
+  int base_stride = 0;
   int record_words = 0;
   int nchunks = 0;
   int max_off = 0;
 };
 
 // delays: [ngroups][ndm_group][rows_per_group] (rows beyond a ragged last
-// group are ignored).  Builds base[group][block][row] and the records.
+// group are ignored).  Builds base[group][block][row] (rows padded to a
+// multiple of 4, so every chunk's bases start on 16 bytes) and the records.
 Records build_records(const std::vector<int32_t>& delays, int ngroups, int ndm_group,
                       int rows_per_group, int total_rows, int dms_per_cta, int chunk_rows,
                       int row_bytes) {
@@ -556,7 +592,9 @@ Records build_records(const std::vector<int32_t>& delays, int ngroups, int ndm_g
   const int blocks = static_cast<int>(ceil_div(ndm_group, dms_per_cta));
   r.nchunks = static_cast<int>(ceil_div(rows_per_group, chunk_rows));
   r.record_words = static_cast<int>(round_up(1 + (chunk_rows + 4) / 2, 4));
-  r.base.assign(static_cast<size_t>(ngroups) * blocks * rows_per_group, 0);
+  r.base_stride = static_cast<int>(round_up(rows_per_group, 4));
+  // + 64 entries: the last chunk's 16-byte base copy may read past its block
+  r.base.assign(static_cast<size_t>(ngroups) * blocks * r.base_stride + 64, 0);
   r.words.assign(static_cast<size_t>(ngroups) * ndm_group * r.nchunks * r.record_words, 0u);
   std::vector<uint16_t> cls[4];
   for (int g = 0; g < ngroups; ++g) {
@@ -565,7 +603,7 @@ Records build_records(const std::vector<int32_t>& delays, int ngroups, int ndm_g
       const int d0 = b * dms_per_cta;
       for (int row = 0; row < grows; ++row) {
         const int32_t d = delays[(static_cast<size_t>(g) * ndm_group + d0) * rows_per_group + row];
-        r.base[(static_cast<size_t>(g) * blocks + b) * rows_per_group + row] = d & ~15;
+        r.base[(static_cast<size_t>(g) * blocks + b) * r.base_stride + row] = d & ~15;
       }
     }
     for (int dm = 0; dm < ndm_group; ++dm) {
@@ -577,7 +615,7 @@ Records build_records(const std::vector<int32_t>& delays, int ngroups, int ndm_g
         for (int i = 0; i < nrows; ++i) {
           const int row = row0 + i;
           const int32_t d = delays[(static_cast<size_t>(g) * ndm_group + dm) * rows_per_group + row];
-          const int32_t off = d - r.base[(static_cast<size_t>(g) * blocks + b) * rows_per_group + row];
+          const int32_t off = d - r.base[(static_cast<size_t>(g) * blocks + b) * r.base_stride + row];
           r.max_off = std::max(r.max_off, off);
           const int word = i * (row_bytes / 4) + (off >> 2);
           cls[off & 3].push_back(static_cast<uint16_t>(word));
@@ -620,7 +658,8 @@ struct Launch {
 // every shape gives the same sums.
 template <typename F>
 Launch choose_launch(F&& max_off_for, int dpc_fix, int cr_fix) {
-  const size_t budget2 = 112 * 1024, budget1 = 224 * 1024;
+  const size_t acc = static_cast<size_t>(kWarps) * kWords * 4 * 32 * 4;  // 32-bit sums
+  const size_t budget2 = 112 * 1024 - acc, budget1 = 224 * 1024 - acc;
   for (size_t budget : {budget2, budget1}) {
     for (int dpc : {8, 4, 2, 1}) {
       if (dpc_fix && dpc != dpc_fix) continue;
@@ -630,11 +669,11 @@ Launch choose_launch(F&& max_off_for, int dpc_fix, int cr_fix) {
       for (int cr : {64, 32, 16, 8}) {
         if (cr_fix && cr != cr_fix) continue;
         const size_t rec = static_cast<size_t>(dpc) * round_up(1 + (cr + 4) / 2, 4) * 4;
-        const size_t stage = static_cast<size_t>(cr) * row_bytes + rec;
+        const size_t stage = static_cast<size_t>(cr) * row_bytes + rec + round_up(cr * 4, 16);
         if (static_cast<size_t>(cr) * row_bytes >= 65536 * 4) continue;  // u16 word offsets
         for (int st : {3, 2}) {
           if (st * stage <= budget)
-            return Launch{dpc, wpd, cr, row_bytes, st, static_cast<uint32_t>(stage), st * stage};
+            return Launch{dpc, wpd, cr, row_bytes, st, static_cast<uint32_t>(stage), st * stage + acc};
         }
       }
     }
@@ -715,9 +754,10 @@ struct BytesStage {
     p.in_valid = valid;
     p.rows_per_group = rows_per_group;
     p.total_rows = total_rows - g0 * rows_per_group;
-    p.base_group_stride = static_cast<uint64_t>(blocks) * rows_per_group;
+    p.base_block_stride = static_cast<uint64_t>(rec.base_stride);
+    p.base_group_stride = static_cast<uint64_t>(blocks) * p.base_block_stride;
     p.base = base_dev.as<int32_t>() + g0 * p.base_group_stride +
-             static_cast<uint64_t>(dm_first / launch.dms_per_cta) * rows_per_group;
+             static_cast<uint64_t>(dm_first / launch.dms_per_cta) * p.base_block_stride;
     p.rec_dm_stride = static_cast<uint64_t>(rec.nchunks) * rec.record_words;
     p.rec_group_stride = static_cast<uint64_t>(ndm_group) * p.rec_dm_stride;
     p.records = rec_dev.as<uint32_t>() + g0 * p.rec_group_stride + dm_first * p.rec_dm_stride;
@@ -744,6 +784,7 @@ struct BytesStage {
     p.grid_x = static_cast<uint32_t>(ctas);
     p.stages = launch.stages;
     p.stage_bytes = launch.stage_bytes;
+    p.base_bytes = static_cast<uint32_t>(round_up(launch.chunk_rows * 4, 16));
     p.status = status_dev.as<uint32_t>();
     return p;
   }

@@ -92,12 +92,13 @@ struct OctaveDev {
 // prepare: all octaves in one pass over the series
 // ---------------------------------------------------------------------------
 
+// (the series and statistics are read-only during the prepare launch)
 __device__ __forceinline__ float normalised(const float* row, uint64_t i, const double* stats) {
-  const float y = row[i];
+  const float y = __ldg(row + i);
   if (stats == nullptr) return y;
-  const double scale = stats[1];
+  const double scale = __ldg(stats + 1);
   if (scale == 0.0) return 0.0f;
-  return static_cast<float>(__dmul_rn(__dsub_rn(static_cast<double>(y), stats[0]), scale));
+  return static_cast<float>(__dmul_rn(__dsub_rn(static_cast<double>(y), __ldg(stats)), scale));
 }
 
 // first output index k with floor(k * f) >= x (k * f evaluated as the
@@ -109,17 +110,61 @@ __device__ __forceinline__ uint64_t first_output_at(uint64_t x, double f) {
   return k;
 }
 
-__global__ void __launch_bounds__(kThreads) prepare_kernel(const float* __restrict__ series, uint64_t stride,
-                                                           uint64_t n, const double* __restrict__ stats,
-                                                           const OctaveDev* __restrict__ octaves, int noct,
-                                                           uint64_t halo, float* __restrict__ prepared,
-                                                           uint64_t prep_stride) {
+// One member's series in a prepare launch.
+struct PrepareItem {
+  const float* series;
+  uint64_t stride, n;
+  const double* stats;      // null: no normalisation
+  const OctaveDev* octaves;
+  int32_t noct;
+  uint32_t nseries;
+  uint64_t halo;
+  float* prepared;
+  uint64_t prep_stride;
+};
+
+// The items of a prepare launch: a device table (batched) or one by value.
+struct PrepareTable {
+  const PrepareItem* items;  // null: `one` only
+  const uint64_t* begin;     // first CTA of each item
+  int32_t nitems;
+  PrepareItem one;
+};
+
+uint64_t prepare_ctas(const PrepareItem& it) { return ceil_div(it.n, kPrepareChunk) * it.nseries; }
+
+template <bool Batched>
+__global__ void __launch_bounds__(kThreads) prepare_kernel(const __grid_constant__ PrepareTable tab) {
   extern __shared__ float xs[];
   __shared__ uint64_t kb[32], cnt_prefix[33];
-  const int s = blockIdx.y;
-  const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kPrepareChunk;
-  const float* row = series + s * stride;
-  const double* st = stats ? stats + 2 * s : nullptr;
+  __shared__ PrepareItem sit;
+  __shared__ uint32_t sloc;
+  // a single-item launch reads the parameter; a batched one shares thread 0's
+  // lookup (the last item starting at or before the CTA)
+  uint32_t local = blockIdx.x;
+  if (Batched) {
+    if (threadIdx.x == 0) {
+      const uint64_t b = blockIdx.x;
+      int lo = 0, hi = tab.nitems;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (tab.begin[mid] <= b) lo = mid; else hi = mid;
+      }
+      sit = tab.items[lo];
+      sloc = static_cast<uint32_t>(b - tab.begin[lo]);
+    }
+    __syncthreads();
+    local = sloc;
+  }
+  const PrepareItem& it = Batched ? sit : tab.one;
+  const uint64_t n = it.n, halo = it.halo;
+  const OctaveDev* octaves = it.octaves;
+  const int noct = it.noct;
+  const uint32_t xblocks = static_cast<uint32_t>(ceil_div(n, kPrepareChunk));
+  const uint64_t s = local / xblocks;
+  const uint64_t c0 = static_cast<uint64_t>(local % xblocks) * kPrepareChunk;
+  const float* __restrict__ row = it.series + s * it.stride;
+  const double* st = it.stats ? it.stats + 2 * s : nullptr;
   const uint64_t span = umin64(kPrepareChunk + halo, n - c0);
   for (uint64_t i = threadIdx.x; i < span; i += kThreads) xs[i] = normalised(row, c0 + i, st);
   if (threadIdx.x == 0) {
@@ -141,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) prepare_kernel(const float* __restri
   }
   __syncthreads();
   const uint64_t total = cnt_prefix[noct];
-  float* out_row = prepared + s * prep_stride;
+  float* __restrict__ out_row = it.prepared + s * it.prep_stride;
   const double last_index = static_cast<double>(n - 1);
   for (uint64_t idx = threadIdx.x; idx < total; idx += kThreads) {
     int o = 0;
@@ -775,6 +820,9 @@ struct gf_ffa_program {
   uint64_t max_series = 0;
   uint64_t scratch_floats = 0;
   DeviceBlob tasks_d, trials_d, sub_meta_d, sub_offset_d, col_meta_d, blocks_d, passes_d, members_d;
+  // batched prepare of every member (gf_ffa_batch_bind_series)
+  DeviceBlob prepare_items_d, prepare_begin_d;
+  uint64_t prepare_ctas_total = 0, prepare_halo = 0;
 };
 
 namespace {
@@ -1205,22 +1253,44 @@ std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& spe
   return P;
 }
 
-void launch_prepare(const gf_ffa_program* P, const FfaMember& M, const float* dev_series, uint64_t nseries,
-                    uint64_t stride, const double* dev_stats, float* dev_prepared, cudaStream_t s) {
+PrepareItem prepare_item(const FfaMember& M, const float* dev_series, uint64_t nseries, uint64_t stride,
+                         const double* dev_stats, float* dev_prepared) {
   check_arg(dev_series && dev_prepared, "null argument");
-  check_arg(nseries > 0 && nseries < 65536, "nseries out of range");
+  check_arg(nseries > 0 && nseries < (1ull << 31), "nseries out of range");
   check_arg(stride >= M.nsamples, "stride must be >= nsamples");
-  DeviceGuard dg(P->device);
-  const size_t smem = (kPrepareChunk + M.halo) * sizeof(float);
-  check_arg(smem <= 200 * 1024, "downsample factor too large for the prepare kernel");
-  cuda_check(cudaFuncSetAttribute(prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  check_arg((kPrepareChunk + M.halo) * sizeof(float) <= 200 * 1024,
+            "downsample factor too large for the prepare kernel");
+  PrepareItem it{};
+  it.series = dev_series;
+  it.stride = stride;
+  it.n = M.nsamples;
+  it.stats = dev_stats;
+  it.octaves = M.octaves_d.as<OctaveDev>();
+  it.noct = static_cast<int32_t>(M.octaves.size());
+  it.nseries = static_cast<uint32_t>(nseries);
+  it.halo = M.halo;
+  it.prepared = dev_prepared;
+  it.prep_stride = M.prep_stride;
+  return it;
+}
+
+template <bool Batched>
+void launch_prepare_table(const PrepareTable& tab, uint64_t ctas, uint64_t halo, cudaStream_t s) {
+  const size_t smem = (kPrepareChunk + halo) * sizeof(float);
+  check_arg(ctas < (1ull << 31), "prepare launch too large");
+  cuda_check(cudaFuncSetAttribute(prepare_kernel<Batched>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)),
              "cudaFuncSetAttribute(prepare_kernel)");
-  dim3 grid(static_cast<unsigned>(ceil_div(M.nsamples, kPrepareChunk)), static_cast<unsigned>(nseries));
-  prepare_kernel<<<grid, kThreads, smem, s>>>(dev_series, stride, M.nsamples, dev_stats,
-                                              M.octaves_d.as<OctaveDev>(), static_cast<int>(M.octaves.size()),
-                                              M.halo, dev_prepared, M.prep_stride);
+  prepare_kernel<Batched><<<static_cast<unsigned>(ctas), kThreads, smem, s>>>(tab);
   cuda_check(cudaGetLastError(), "prepare_kernel launch");
+}
+
+void launch_prepare(const gf_ffa_program* P, const FfaMember& M, const float* dev_series, uint64_t nseries,
+                    uint64_t stride, const double* dev_stats, float* dev_prepared, cudaStream_t s) {
+  DeviceGuard dg(P->device);
+  PrepareTable tab{};
+  tab.one = prepare_item(M, dev_series, nseries, stride, dev_stats, dev_prepared);
+  launch_prepare_table<false>(tab, prepare_ctas(tab.one), M.halo, s);
 }
 
 // One launch per class; batched programs walk their item runs.
@@ -1446,6 +1516,43 @@ extern "C" int gf_ffa_batch_prepare(gf_ffa_program* P, uint64_t member, const fl
     const FfaMember& M = P->members[member];
     launch_prepare(P, M, dev_series, M.nseries, stride, dev_stats, const_cast<float*>(M.prepared),
                    as_stream(stream));
+  });
+}
+
+extern "C" int gf_ffa_batch_bind_series(gf_ffa_program* P, const float* const* dev_series, const uint64_t* strides,
+                                        const double* const* dev_stats) {
+  return guarded([&] {
+    check_arg(P && dev_series && strides, "null argument");
+    check_arg(P->batched && P->bound, "gf_ffa_batch_bind_series needs a bound batched FFA program");
+    DeviceGuard dg(P->device);
+    std::vector<PrepareItem> items;
+    std::vector<uint64_t> begin;
+    uint64_t total = 0, halo = 0;
+    for (size_t m = 0; m < P->members.size(); ++m) {
+      const FfaMember& M = P->members[m];
+      items.push_back(prepare_item(M, dev_series[m], M.nseries, strides[m], dev_stats ? dev_stats[m] : nullptr,
+                                   const_cast<float*>(M.prepared)));
+      begin.push_back(total);
+      total += prepare_ctas(items.back());
+      halo = std::max(halo, M.halo);
+    }
+    P->prepare_items_d.upload(items.data(), items.size() * sizeof(PrepareItem), P->device);
+    P->prepare_begin_d.upload(begin.data(), begin.size() * sizeof(uint64_t), P->device);
+    P->prepare_ctas_total = total;
+    P->prepare_halo = halo;
+  });
+}
+
+extern "C" int gf_ffa_batch_prepare_all(gf_ffa_program* P, void* stream) {
+  return guarded([&] {
+    check_arg(P != nullptr, "null argument");
+    check_arg(P->prepare_items_d.ptr != nullptr, "gf_ffa_batch_prepare_all needs gf_ffa_batch_bind_series");
+    DeviceGuard dg(P->device);
+    PrepareTable tab{};
+    tab.items = P->prepare_items_d.as<PrepareItem>();
+    tab.begin = P->prepare_begin_d.as<uint64_t>();
+    tab.nitems = static_cast<int32_t>(P->members.size());
+    launch_prepare_table<true>(tab, P->prepare_ctas_total, P->prepare_halo, as_stream(stream));
   });
 }
 

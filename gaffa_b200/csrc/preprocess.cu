@@ -18,28 +18,107 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
+#include <vector>
 
 namespace gf {
 namespace {
 
 constexpr int kMaxMedianWindow = 2047;
+constexpr int kMedianWarps = 4;
+constexpr int kStatsWarps = 4;
 
-template <bool U32>
-__device__ __forceinline__ float load_sample(const void* base, uint64_t i) {
-  if (U32) return static_cast<float>(static_cast<const uint32_t*>(base)[i]);
+__device__ __forceinline__ float load_sample(const void* base, uint64_t i, bool u32) {
+  if (u32) return static_cast<float>(static_cast<const uint32_t*>(base)[i]);
   return static_cast<const float*>(base)[i];
+}
+// for inputs no thread of the launch writes (scrunch and median inputs)
+__device__ __forceinline__ float load_sample_ro(const void* base, uint64_t i, bool u32) {
+  if (u32) return static_cast<float>(__ldg(static_cast<const uint32_t*>(base) + i));
+  return __ldg(static_cast<const float*>(base) + i);
+}
+
+// One set of series of one length in a preprocessing launch: the arguments of
+// gf_preprocess_inplace evaluated for every stage.
+struct PrepItem {
+  void* series;         // [nseries][stride] uint32 or float, detrended in place
+  uint64_t stride, n;
+  uint64_t factor, low_n, low_stride;
+  float* low;           // scrunched series [nseries][low_stride] (factor > 1)
+  float* lowmed;        // running median [nseries][low_stride]
+  double* stats;        // [nseries][2]
+  uint32_t* status;
+  uint32_t nseries;
+  int32_t w;            // median window (odd)
+  int32_t u32;          // series holds uint32 sums
+  int32_t normalise, reject_constant;
+  int32_t reserved;
+};
+
+enum PrepStage { kScrunch = 0, kMedian, kDetrend, kStats, kStages };
+
+// CTAs of an item in each stage's launch.
+uint64_t stage_ctas(const PrepItem& it, int stage) {
+  switch (stage) {
+    case kScrunch: return it.factor > 1 ? ceil_div(it.low_n, 128) * it.nseries : 0;
+    case kMedian: return ceil_div(it.nseries, kMedianWarps);
+    case kDetrend: return ceil_div(it.n, 256) * it.nseries;
+    default: return ceil_div(it.nseries, kStatsWarps);
+  }
+}
+
+// The items of a launch: a device table (batched) or one item by value.
+struct PrepTable {
+  const PrepItem* items;   // null: `one` is the launch's only item
+  const uint64_t* begin;   // [kStages][nitems]: first CTA of each item in each stage
+  int32_t nitems;
+  PrepItem one;
+};
+
+// The item of this CTA and the CTA's index inside it.  A single-item launch
+// (Batched = false) reads the kernel parameter directly; a batched one has
+// thread 0 find the item (the last one starting at or before the CTA) and
+// share a copy.  Launches stay below 2^31 CTAs, so CTA indices are 32-bit.
+template <bool Batched>
+__device__ __forceinline__ const PrepItem& cta_item(const PrepTable& t, int stage, PrepItem& shared_it,
+                                                    uint32_t& shared_local, uint32_t& local) {
+  if (!Batched) {
+    local = blockIdx.x;
+    return t.one;
+  }
+  if (threadIdx.x == 0) {
+    const uint64_t b = blockIdx.x;
+    const uint64_t* begin = t.begin + static_cast<uint64_t>(stage) * t.nitems;
+    int lo = 0, hi = t.nitems;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (begin[mid] <= b) lo = mid; else hi = mid;
+    }
+    shared_it = t.items[lo];
+    shared_local = static_cast<uint32_t>(b - begin[lo]);
+  }
+  __syncthreads();
+  local = shared_local;
+  return shared_it;
 }
 
 // low[s][k] = float(double sum of x[kF .. kF+F) / F); 128 outputs per CTA,
 // staged 32 samples at a time so global loads stay coalesced.
-template <bool U32>
-__global__ void __launch_bounds__(128) scrunch_kernel(const void* __restrict__ series, uint64_t stride,
-                                                      uint64_t factor, uint64_t low_n,
-                                                      float* __restrict__ low, uint64_t low_stride) {
+template <bool Batched>
+__global__ void __launch_bounds__(128) scrunch_kernel(const __grid_constant__ PrepTable tab) {
+  __shared__ PrepItem sit;
+  __shared__ uint32_t sloc;
+  uint32_t local;
+  const PrepItem& it = cta_item<Batched>(tab, kScrunch, sit, sloc, local);
   __shared__ float tile[128][33];
-  const int s = blockIdx.y;
-  const uint64_t k0 = static_cast<uint64_t>(blockIdx.x) * 128;
-  const char* row = static_cast<const char*>(series) + s * stride * 4;
+  const uint32_t xblocks = static_cast<uint32_t>(ceil_div(it.low_n, 128));
+  const uint64_t s = local / xblocks;
+  const uint64_t k0 = static_cast<uint64_t>(local % xblocks) * 128;
+  const uint64_t factor = it.factor, low_n = it.low_n;
+  const bool u32 = it.u32 != 0;
+  float* const low = it.low;
+  const uint64_t low_stride = it.low_stride;
+  const char* row = static_cast<const char*>(it.series) + s * it.stride * 4;
   double acc = 0.0;
   for (uint64_t i0 = 0; i0 < factor; i0 += 32) {
     const int cols = static_cast<int>(umin64(32, factor - i0));
@@ -48,7 +127,7 @@ __global__ void __launch_bounds__(128) scrunch_kernel(const void* __restrict__ s
       const int r = e >> 5, c = e & 31;
       const uint64_t k = k0 + r;
       float v = 0.0f;
-      if (k < low_n && c < cols) v = load_sample<U32>(row, k * factor + i0 + c);
+      if (k < low_n && c < cols) v = load_sample_ro(row, k * factor + i0 + c, u32);
       tile[r][c] = v;
     }
     __syncthreads();
@@ -66,24 +145,33 @@ __global__ void __launch_bounds__(128) scrunch_kernel(const void* __restrict__ s
 // value's rank, and rebuild each slot from its old neighbour (shift by -1, 0
 // or +1).  The upper median of an odd window is its middle element, the same
 // value std::nth_element selects.
-template <bool U32>
-__global__ void __launch_bounds__(128) running_median_kernel(const void* __restrict__ in, uint64_t in_stride,
-                                                             uint64_t n, int w, float* __restrict__ out,
-                                                             uint64_t out_stride, int nseries) {
+// Input: the scrunched series (factor > 1) or the series itself.
+template <bool Batched>
+__global__ void __launch_bounds__(32 * kMedianWarps) running_median_kernel(const __grid_constant__ PrepTable tab) {
+  __shared__ PrepItem sit;
+  __shared__ uint32_t sloc;
+  uint32_t local;
+  const PrepItem& it = cta_item<Batched>(tab, kMedian, sit, sloc, local);
   extern __shared__ float med_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int s = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (s >= nseries) return;
+  const uint64_t s = static_cast<uint64_t>(local) * kMedianWarps + warp;
+  if (s >= it.nseries) return;
+  const bool scrunched = it.factor > 1;
+  const void* in = scrunched ? static_cast<const void*>(it.low) : it.series;
+  const uint64_t in_stride = scrunched ? it.low_stride : it.stride;
+  const uint64_t n = scrunched ? it.low_n : it.n;
+  const bool u32 = !scrunched && it.u32 != 0;
+  const int w = it.w;
   const int cap = ((w + 31) / 32) * 32;
   float* A = med_smem + warp * 2 * cap;
   float* B = A + cap;
-  const char* row = static_cast<const char*>(in) + static_cast<uint64_t>(s) * in_stride * 4;
-  float* orow = out + static_cast<uint64_t>(s) * out_stride;
+  const char* row = static_cast<const char*>(in) + s * in_stride * 4;
+  float* orow = it.lowmed + s * it.low_stride;
   const int half = w / 2;
   auto padded = [&](int64_t j) -> float {
     int64_t i = j - half;
     i = i < 0 ? 0 : (i >= static_cast<int64_t>(n) ? static_cast<int64_t>(n) - 1 : i);
-    return load_sample<U32>(row, static_cast<uint64_t>(i));
+    return load_sample_ro(row, static_cast<uint64_t>(i), u32);
   };
   // initial window, sorted by an odd-even transposition sort over cap slots
   for (int j = lane; j < cap; j += 32) A[j] = j < w ? padded(j) : INFINITY;
@@ -137,21 +225,26 @@ __global__ void __launch_bounds__(128) running_median_kernel(const void* __restr
 }
 
 // y = x - trend, written in place as float (buffer may hold uint32 input).
-template <bool U32, bool Scrunched>
-__global__ void __launch_bounds__(256) detrend_kernel(void* series, uint64_t stride, uint64_t n,
-                                                      const float* __restrict__ lowmed, uint64_t low_stride,
-                                                      uint64_t low_n, uint64_t factor, uint32_t* status) {
-  const int s = blockIdx.y;
-  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  char* row = static_cast<char*>(series) + s * stride * 4;
-  const float* lm = lowmed + s * low_stride;
-  const float x = load_sample<U32>(row, i);
-  if (!U32 && !isfinite(x)) atomicOr(status, GF_STATUS_NONFINITE);
+template <bool Batched>
+__global__ void __launch_bounds__(256) detrend_kernel(const __grid_constant__ PrepTable tab) {
+  __shared__ PrepItem sit;
+  __shared__ uint32_t sloc;
+  uint32_t local;
+  const PrepItem& it = cta_item<Batched>(tab, kDetrend, sit, sloc, local);
+  const uint32_t xblocks = static_cast<uint32_t>(ceil_div(it.n, 256));
+  const uint64_t s = local / xblocks;
+  const uint64_t i = static_cast<uint64_t>(local % xblocks) * 256 + threadIdx.x;
+  if (i >= it.n) return;
+  const bool u32 = it.u32 != 0;
+  char* row = static_cast<char*>(it.series) + s * it.stride * 4;
+  const float* lm = it.lowmed + s * it.low_stride;
+  const float x = load_sample(row, i, u32);
+  if (!u32 && !isfinite(x)) atomicOr(it.status, GF_STATUS_NONFINITE);
   float trend;
-  if (!Scrunched) {
+  if (it.factor == 1) {
     trend = lm[i];
   } else {
+    const uint64_t factor = it.factor, low_n = it.low_n;
     const double offset = 0.5 * static_cast<double>(factor - 1);
     const double pos = __ddiv_rn(__dsub_rn(static_cast<double>(i), offset), static_cast<double>(factor));
     if (pos <= 0.0) {
@@ -175,7 +268,6 @@ __global__ void __launch_bounds__(256) detrend_kernel(void* series, uint64_t str
 // flight) while lane 0 runs the dependent chain sum += y; sq += y * y over the
 // chunk already resident, so the chain never waits on global memory.
 constexpr int kStatsChunk = 1024;  // floats per chunk
-constexpr int kStatsWarps = 4;
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -185,15 +277,18 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
-__global__ void __launch_bounds__(32 * kStatsWarps) stats_kernel(const float* __restrict__ series, uint64_t stride,
-                                                                 uint64_t n, int nseries, int normalise,
-                                                                 int reject_constant, double* __restrict__ stats,
-                                                                 uint32_t* status) {
+template <bool Batched>
+__global__ void __launch_bounds__(32 * kStatsWarps) stats_kernel(const __grid_constant__ PrepTable tab) {
+  __shared__ PrepItem sit;
+  __shared__ uint32_t sloc;
+  uint32_t local;
+  const PrepItem& it = cta_item<Batched>(tab, kStats, sit, sloc, local);
   __shared__ __align__(16) float buf[kStatsWarps][2][kStatsChunk];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int s = blockIdx.x * kStatsWarps + warp;
-  if (s >= nseries) return;
-  const float* row = series + static_cast<uint64_t>(s) * stride;
+  const uint64_t s = static_cast<uint64_t>(local) * kStatsWarps + warp;
+  if (s >= it.nseries) return;
+  const uint64_t n = it.n;
+  const float* row = static_cast<const float*>(it.series) + s * it.stride;
   // vector staging needs 16-byte aligned rows; others take the scalar tail path
   const uint64_t nvec = (reinterpret_cast<uintptr_t>(row) & 15) == 0 ? n / 4 : 0;
   const uint64_t nchunks = (nvec * 4 + kStatsChunk - 1) / kStatsChunk;
@@ -235,17 +330,17 @@ __global__ void __launch_bounds__(32 * kStatsWarps) stats_kernel(const float* __
   if (var < 0.0 && var > -1.0e-12) var = 0.0;
   double scale = 0.0;
   if (!(var >= 0.0) || !isfinite(var)) {
-    atomicOr(status, GF_STATUS_NONFINITE);
+    atomicOr(it.status, GF_STATUS_NONFINITE);
   } else {
     const double sd = __dsqrt_rn(var);
     if (!(sd > 0.0) || !isfinite(sd)) {
-      if (normalise && reject_constant) atomicOr(status, GF_STATUS_CONSTANT);
+      if (it.normalise && it.reject_constant) atomicOr(it.status, GF_STATUS_CONSTANT);
     } else {
       scale = __ddiv_rn(1.0, sd);
     }
   }
-  stats[2 * s] = mean;
-  stats[2 * s + 1] = scale;
+  it.stats[2 * s] = mean;
+  it.stats[2 * s + 1] = scale;
 }
 
 __global__ void __launch_bounds__(256) normalise_kernel(float* series, uint64_t stride, uint64_t n,
@@ -307,64 +402,125 @@ extern "C" int gf_preprocess_info_get(const gf_preprocess_desc* d, gf_preprocess
   });
 }
 
+namespace {
+
+// The launch item of gf_preprocess_inplace's arguments.
+PrepItem make_item(const gf_preprocess_desc& d, void* dev_series, int32_t input_is_u32, uint64_t nseries,
+                   uint64_t stride, void* dev_workspace, double* dev_stats, uint32_t* dev_status) {
+  check_arg(dev_series && dev_workspace && dev_stats && dev_status, "null argument");
+  check_arg(nseries > 0 && nseries <= d.max_series, "nseries must be in (0, max_series]");
+  check_arg(nseries < (1ull << 31), "too many series per call");
+  check_arg(stride >= d.nsamples, "stride must be >= nsamples");
+  const Geometry g = geometry(d);
+  PrepItem it{};
+  it.series = dev_series;
+  it.stride = stride;
+  it.n = d.nsamples;
+  it.factor = g.factor;
+  it.low_n = g.low_n;
+  it.low_stride = g.low_stride;
+  it.low = static_cast<float*>(dev_workspace);
+  it.lowmed = g.factor == 1 ? it.low : it.low + g.low_stride * nseries;
+  it.stats = dev_stats;
+  it.status = dev_status;
+  it.nseries = static_cast<uint32_t>(nseries);
+  it.w = static_cast<int32_t>(g.factor == 1 ? g.window : d.min_points);
+  it.u32 = input_is_u32 ? 1 : 0;
+  it.normalise = d.normalise;
+  it.reject_constant = d.reject_constant;
+  return it;
+}
+
+size_t median_smem(int w) {
+  const int cap = ((w + 31) / 32) * 32;
+  return static_cast<size_t>(kMedianWarps) * 2 * cap * sizeof(float);
+}
+
+// The four stages over a table whose stage grids are ctas[stage].
+template <bool Batched>
+void launch_stages(const PrepTable& tab, const uint64_t (&ctas)[kStages], size_t med_smem, cudaStream_t s) {
+  for (int st = 0; st < kStages; ++st)
+    check_arg(ctas[st] < (1ull << 31), "preprocessing launch too large");
+  cuda_check(cudaFuncSetAttribute(running_median_kernel<Batched>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(med_smem)),
+             "cudaFuncSetAttribute(median)");
+  if (ctas[kScrunch]) scrunch_kernel<Batched><<<static_cast<unsigned>(ctas[kScrunch]), 128, 0, s>>>(tab);
+  running_median_kernel<Batched><<<static_cast<unsigned>(ctas[kMedian]), 32 * kMedianWarps, med_smem, s>>>(tab);
+  cuda_check(cudaGetLastError(), "running median launch");
+  detrend_kernel<Batched><<<static_cast<unsigned>(ctas[kDetrend]), 256, 0, s>>>(tab);
+  cuda_check(cudaGetLastError(), "detrend launch");
+  stats_kernel<Batched><<<static_cast<unsigned>(ctas[kStats]), 32 * kStatsWarps, 0, s>>>(tab);
+  cuda_check(cudaGetLastError(), "stats launch");
+}
+
+}  // namespace
+
 extern "C" int gf_preprocess_inplace(const gf_preprocess_desc* d, void* dev_series, int32_t input_is_u32,
                                      uint64_t nseries, uint64_t stride, void* dev_workspace,
                                      double* dev_stats, uint32_t* dev_status, void* stream) {
   return guarded([&] {
-    check_arg(d && dev_series && dev_workspace && dev_stats && dev_status, "null argument");
-    check_arg(nseries > 0 && nseries <= d->max_series, "nseries must be in (0, max_series]");
-    check_arg(nseries < 65536, "at most 65535 series per call");
-    check_arg(stride >= d->nsamples, "stride must be >= nsamples");
-    const Geometry g = geometry(*d);
-    auto s = as_stream(stream);
-    const uint64_t n = d->nsamples;
-    float* low = static_cast<float*>(dev_workspace);
-    float* lowmed = g.factor == 1 ? low : low + g.low_stride * nseries;
-    const int w = static_cast<int>(g.factor == 1 ? g.window : d->min_points);
-    const int cap = ((w + 31) / 32) * 32;
-    const int warps = 4;
-    const size_t med_smem = static_cast<size_t>(warps) * 2 * cap * sizeof(float);
-    const unsigned med_grid = static_cast<unsigned>(ceil_div(nseries, warps));
-    const unsigned rows = static_cast<unsigned>(nseries);
-    cuda_check(cudaFuncSetAttribute(running_median_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(med_smem)), "cudaFuncSetAttribute(median)");
-    cuda_check(cudaFuncSetAttribute(running_median_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(med_smem)), "cudaFuncSetAttribute(median)");
-    if (g.factor > 1) {
-      dim3 sg(static_cast<unsigned>(ceil_div(g.low_n, 128)), rows);
-      if (input_is_u32)
-        scrunch_kernel<true><<<sg, 128, 0, s>>>(dev_series, stride, g.factor, g.low_n, low, g.low_stride);
-      else
-        scrunch_kernel<false><<<sg, 128, 0, s>>>(dev_series, stride, g.factor, g.low_n, low, g.low_stride);
-      running_median_kernel<false><<<med_grid, warps * 32, med_smem, s>>>(low, g.low_stride, g.low_n, w, lowmed,
-                                                                          g.low_stride, static_cast<int>(nseries));
-    } else {
-      if (input_is_u32)
-        running_median_kernel<true><<<med_grid, warps * 32, med_smem, s>>>(dev_series, stride, n, w, lowmed,
-                                                                           g.low_stride, static_cast<int>(nseries));
-      else
-        running_median_kernel<false><<<med_grid, warps * 32, med_smem, s>>>(dev_series, stride, n, w, lowmed,
-                                                                            g.low_stride, static_cast<int>(nseries));
-    }
-    cuda_check(cudaGetLastError(), "running median launch");
-    dim3 dg(static_cast<unsigned>(ceil_div(n, 256)), rows);
-    if (input_is_u32) {
-      if (g.factor > 1)
-        detrend_kernel<true, true><<<dg, 256, 0, s>>>(dev_series, stride, n, lowmed, g.low_stride, g.low_n, g.factor, dev_status);
-      else
-        detrend_kernel<true, false><<<dg, 256, 0, s>>>(dev_series, stride, n, lowmed, g.low_stride, g.low_n, g.factor, dev_status);
-    } else {
-      if (g.factor > 1)
-        detrend_kernel<false, true><<<dg, 256, 0, s>>>(dev_series, stride, n, lowmed, g.low_stride, g.low_n, g.factor, dev_status);
-      else
-        detrend_kernel<false, false><<<dg, 256, 0, s>>>(dev_series, stride, n, lowmed, g.low_stride, g.low_n, g.factor, dev_status);
-    }
-    cuda_check(cudaGetLastError(), "detrend launch");
-    stats_kernel<<<static_cast<unsigned>(ceil_div(nseries, kStatsWarps)), 32 * kStatsWarps, 0, s>>>(
-        static_cast<const float*>(dev_series), stride, n, static_cast<int>(nseries), d->normalise,
-        d->reject_constant, dev_stats, dev_status);
-    cuda_check(cudaGetLastError(), "stats launch");
+    check_arg(d != nullptr, "null argument");
+    PrepTable tab{};
+    tab.one = make_item(*d, dev_series, input_is_u32, nseries, stride, dev_workspace, dev_stats, dev_status);
+    uint64_t ctas[kStages];
+    for (int st = 0; st < kStages; ++st) ctas[st] = stage_ctas(tab.one, st);
+    launch_stages<false>(tab, ctas, median_smem(tab.one.w), as_stream(stream));
   });
+}
+
+// Many gf_preprocess_inplace calls (series of different lengths and options)
+// as one launch per stage.
+struct gf_preprocess_batch {
+  int device = 0;
+  int nitems = 0;
+  uint64_t ctas[kStages] = {0, 0, 0, 0};
+  size_t med_smem = 0;
+  DeviceBlob items_d, begin_d;
+};
+
+extern "C" int gf_preprocess_batch_create(const gf_preprocess_batch_item* items, uint64_t nitems,
+                                          int32_t device_id, gf_preprocess_batch** out) {
+  return guarded([&] {
+    check_arg(items && out, "null argument");
+    *out = nullptr;
+    check_arg(nitems > 0 && nitems < (1u << 20), "batched preprocessing takes 1 to 2^20 items");
+    auto B = std::make_unique<gf_preprocess_batch>();
+    B->device = device_id;
+    B->nitems = static_cast<int>(nitems);
+    std::vector<PrepItem> its;
+    std::vector<uint64_t> begin(kStages * nitems);
+    for (uint64_t i = 0; i < nitems; ++i) {
+      const gf_preprocess_batch_item& x = items[i];
+      check_arg(x.desc != nullptr, "null argument");
+      its.push_back(make_item(*x.desc, x.dev_series, x.input_is_u32, x.nseries, x.stride, x.dev_workspace,
+                              x.dev_stats, x.dev_status));
+      B->med_smem = std::max(B->med_smem, median_smem(its.back().w));
+      for (int st = 0; st < kStages; ++st) {
+        begin[st * nitems + i] = B->ctas[st];
+        B->ctas[st] += stage_ctas(its.back(), st);
+      }
+    }
+    DeviceGuard dg(device_id);
+    B->items_d.upload(its.data(), its.size() * sizeof(PrepItem), device_id);
+    B->begin_d.upload(begin.data(), begin.size() * sizeof(uint64_t), device_id);
+    *out = B.release();
+  });
+}
+
+extern "C" int gf_preprocess_batch_run(gf_preprocess_batch* B, void* stream) {
+  return guarded([&] {
+    check_arg(B != nullptr, "null argument");
+    DeviceGuard dg(B->device);
+    PrepTable tab{};
+    tab.items = B->items_d.as<PrepItem>();
+    tab.begin = B->begin_d.as<uint64_t>();
+    tab.nitems = B->nitems;
+    launch_stages<true>(tab, B->ctas, B->med_smem, as_stream(stream));
+  });
+}
+
+extern "C" int gf_preprocess_batch_destroy(gf_preprocess_batch* B) {
+  return guarded([&] { delete B; });
 }
 
 extern "C" int gf_normalise(float* dev_series, uint64_t nseries, uint64_t stride, uint64_t nsamples,

@@ -295,6 +295,30 @@ int gf_preprocess_inplace(const gf_preprocess_desc* desc, void* dev_series,
                           int32_t input_is_u32, uint64_t nseries, uint64_t stride,
                           void* dev_workspace, double* dev_stats,
                           uint32_t* dev_status, void* stream);
+/* Many gf_preprocess_inplace calls (series sets of different lengths,
+ * windows and options) as one launch per stage: the per-set launches of
+ * preprocess_time_series_batch_inplace_cuda (preprocessing_cuda.cu:819-864),
+ * one per observation in the reference, fill the GPU together.  Each item's
+ * results equal gf_preprocess_inplace with the same arguments.  Pointers are
+ * fixed at creation, so gf_preprocess_batch_run can be captured in a CUDA
+ * graph. */
+typedef struct gf_preprocess_batch gf_preprocess_batch;
+typedef struct {
+  const gf_preprocess_desc* desc;   /* read at creation */
+  void* dev_series;
+  int32_t input_is_u32;
+  int32_t reserved;
+  uint64_t nseries;
+  uint64_t stride;
+  void* dev_workspace;
+  double* dev_stats;
+  uint32_t* dev_status;
+} gf_preprocess_batch_item;
+int gf_preprocess_batch_create(const gf_preprocess_batch_item* items, uint64_t nitems,
+                               int32_t device_id, gf_preprocess_batch** out);
+int gf_preprocess_batch_run(gf_preprocess_batch* batch, void* stream);
+int gf_preprocess_batch_destroy(gf_preprocess_batch* batch);
+
 /* x <- float((x - mean) * (1/stddev)) (time_series.cpp:98-103); zeroes
  * constant series when reject_constant == 0. */
 int gf_normalise(float* dev_series, uint64_t nseries, uint64_t stride,
@@ -426,6 +450,14 @@ int gf_ffa_batch_bind(gf_ffa_program* program, const float* const* dev_prepared)
 int gf_ffa_batch_prepare(gf_ffa_program* program, uint64_t member,
                          const float* dev_series, uint64_t stride,
                          const double* dev_stats, void* stream);
+/* The series gf_ffa_batch_prepare_all reads, for every member m:
+ * dev_series[m] ([nseries][strides[m]] floats) and dev_stats[m] (the
+ * member's gf_preprocess_inplace statistics; dev_stats or an entry may be
+ * null: no normalisation).  Synchronous upload; call before capturing. */
+int gf_ffa_batch_bind_series(gf_ffa_program* program, const float* const* dev_series,
+                             const uint64_t* strides, const double* const* dev_stats);
+/* gf_ffa_batch_prepare of every member in one launch. */
+int gf_ffa_batch_prepare_all(gf_ffa_program* program, void* stream);
 /* One launch per class over every member; no host synchronisation. */
 int gf_ffa_batch_search(gf_ffa_program* program, float snr_threshold,
                         void* dev_scratch, gf_peak_record* dev_peaks,

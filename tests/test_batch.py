@@ -198,6 +198,57 @@ def test_ffa_batch_matches_one_program_per_plan():
     assert _records_key(got) == sorted(want)
 
 
+@pytest.mark.gpu
+def test_preprocess_batch_and_prepare_all_match_single_launches():
+    """One launch per preprocessing stage over series sets of different
+    lengths, windows (scrunched and exact medians) and input types, and one
+    prepare over every member, equal the per-set launches bit for bit."""
+    torch = _cuda()
+    from gaffa_b200 import core
+    gen = torch.Generator(device="cuda").manual_seed(9)
+    # (nsamples, tsamp, window_seconds, min_points, nseries, uint32 input)
+    specs = [(40_000, 64e-6, 0.05, 101, 3, True), (131_072, 64e-6, 1.0, 101, 5, True),
+             (70_001, 128e-6, 0.1, 51, 2, False), (9_000, 64e-6, 0.02, 301, 4, True)]
+    pres, bufs, want = [], [], []
+    for n, ts, win, mp, ns, u32 in specs:
+        pre = core.PreprocessProgram(n, ts, window_seconds=win, min_points=mp, max_series=ns)
+        stride = (n + 3) // 4 * 4 + 4
+        if u32:
+            x = torch.randint(0, 60_000, (ns, stride), generator=gen, device="cuda", dtype=torch.int32)
+        else:
+            x = torch.randn((ns, stride), generator=gen, device="cuda") * 3.0 + 7.0
+        ref = x.clone()
+        stats = pre.run(ref, ns).clone()
+        pre.synchronize()
+        want.append((ref[:, :n].clone(), stats))
+        pres.append(pre)
+        bufs.append(x)
+    assert any(int(p.info.scrunch_factor) > 1 for p in pres) and any(int(p.info.scrunch_factor) == 1 for p in pres)
+    batch = core.PreprocessBatch((p, b, spec[4]) for p, b, spec in zip(pres, bufs, specs))
+    batch.run()
+    for p in pres:
+        p.synchronize()
+    for (n, *_), b, p, (ref, stats) in zip(specs, bufs, pres, want):
+        assert torch.equal(b[:, :n], ref)
+        assert torch.equal(p.stats[: b.shape[0]], stats)
+    # the prepared FFA inputs of every member in one launch
+    plans = [core.make_riptide_ffa_plan(n, ts, 0.05, 0.5, bins_min=48, bins_max=80, duty_cycle_max=0.1)
+             for n, ts, *_ in specs]
+    one = core.FfaBatchProgram([(pl, spec[4]) for pl, spec in zip(plans, specs)])
+    two = core.FfaBatchProgram([(pl, spec[4]) for pl, spec in zip(plans, specs)])
+    for t in one.prepared + two.prepared:
+        t.zero_()  # padding between octaves is never written
+    views = [b.view(torch.float32) for b in bufs]
+    for m, (v, p) in enumerate(zip(views, pres)):
+        one.prepare(m, v, p.stats[: v.shape[0]])
+    two.bind_series(views, [p.stats[: v.shape[0]] for v, p in zip(views, pres)])
+    two.prepare_all()
+    torch.cuda.synchronize()
+    for a, b, mi in zip(one.prepared, two.prepared, one.member_info):
+        k = int(mi.nseries) * int(mi.prepared_floats)
+        assert torch.equal(a.reshape(-1)[:k], b.reshape(-1)[:k])
+
+
 def _assert_same_result(a, b):
     assert np.array_equal(a.peaks, b.peaks)
     assert np.array_equal(a.candidates, b.candidates)
