@@ -653,7 +653,7 @@ struct Launch {
 // Picks the DM block size, channel chunk and ring depth so the stages fit in
 // shared memory with two CTAs per SM when possible (228 KB per SM, 1 KB
 // reserved per CTA, the ring state and batch table in static shared memory):
-// the largest chunk with 3 stages, else with 2.  dpc_fix / cr_fix (0 = any)
+// the largest chunk with 4 stages, else 3, else 2.  dpc_fix / cr_fix (0 = any)
 // pin the DM block or the chunk rows (launch shapes picked by an autotuner);
 // every shape gives the same sums.
 template <typename F>
@@ -671,7 +671,7 @@ Launch choose_launch(F&& max_off_for, int dpc_fix, int cr_fix) {
         const size_t rec = static_cast<size_t>(dpc) * round_up(1 + (cr + 4) / 2, 4) * 4;
         const size_t stage = static_cast<size_t>(cr) * row_bytes + rec + round_up(cr * 4, 16);
         if (static_cast<size_t>(cr) * row_bytes >= 65536 * 4) continue;  // u16 word offsets
-        for (int st : {3, 2}) {
+        for (int st : {4, 3, 2}) {
           if (st * stage <= budget)
             return Launch{dpc, wpd, cr, row_bytes, st, static_cast<uint32_t>(stage), st * stage + acc};
         }

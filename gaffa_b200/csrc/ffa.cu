@@ -92,15 +92,6 @@ struct OctaveDev {
 // prepare: all octaves in one pass over the series
 // ---------------------------------------------------------------------------
 
-// (the series and statistics are read-only during the prepare launch)
-__device__ __forceinline__ float normalised(const float* row, uint64_t i, const double* stats) {
-  const float y = __ldg(row + i);
-  if (stats == nullptr) return y;
-  const double scale = __ldg(stats + 1);
-  if (scale == 0.0) return 0.0f;
-  return static_cast<float>(__dmul_rn(__dsub_rn(static_cast<double>(y), __ldg(stats)), scale));
-}
-
 // first output index k with floor(k * f) >= x (k * f evaluated as the
 // reference does, (double)k * factor)
 __device__ __forceinline__ uint64_t first_output_at(uint64_t x, double f) {
@@ -160,13 +151,25 @@ __global__ void __launch_bounds__(kThreads) prepare_kernel(const __grid_constant
   const uint64_t n = it.n, halo = it.halo;
   const OctaveDev* octaves = it.octaves;
   const int noct = it.noct;
-  const uint32_t xblocks = static_cast<uint32_t>(ceil_div(n, kPrepareChunk));
-  const uint64_t s = local / xblocks;
-  const uint64_t c0 = static_cast<uint64_t>(local % xblocks) * kPrepareChunk;
+  uint64_t s, c0;
+  if (Batched) {
+    const uint32_t xblocks = static_cast<uint32_t>(ceil_div(n, kPrepareChunk));
+    s = local / xblocks;
+    c0 = static_cast<uint64_t>(local % xblocks) * kPrepareChunk;
+  } else {
+    s = blockIdx.y;
+    c0 = static_cast<uint64_t>(blockIdx.x) * kPrepareChunk;
+  }
   const float* __restrict__ row = it.series + s * it.stride;
-  const double* st = it.stats ? it.stats + 2 * s : nullptr;
+  // the series' mean and 1/stddev, loaded once (scale 0: a rejected series)
+  const bool norm = it.stats != nullptr;
+  const double mean = norm ? __ldg(it.stats + 2 * s) : 0.0;
+  const double scale = norm ? __ldg(it.stats + 2 * s + 1) : 1.0;
   const uint64_t span = umin64(kPrepareChunk + halo, n - c0);
-  for (uint64_t i = threadIdx.x; i < span; i += kThreads) xs[i] = normalised(row, c0 + i, st);
+  for (uint64_t i = threadIdx.x; i < span; i += kThreads) {
+    const float y = __ldg(row + c0 + i);
+    xs[i] = !norm ? y : scale == 0.0 ? 0.0f : static_cast<float>(__dmul_rn(__dsub_rn(static_cast<double>(y), mean), scale));
+  }
   if (threadIdx.x == 0) {
     cnt_prefix[0] = 0;
     for (int o = 0; o < noct; ++o) {
@@ -1274,6 +1277,7 @@ PrepareItem prepare_item(const FfaMember& M, const float* dev_series, uint64_t n
   return it;
 }
 
+// Batched: `ctas` CTAs over the table; single: (chunks, series) grid, ctas = chunks.
 template <bool Batched>
 void launch_prepare_table(const PrepareTable& tab, uint64_t ctas, uint64_t halo, cudaStream_t s) {
   const size_t smem = (kPrepareChunk + halo) * sizeof(float);
@@ -1281,7 +1285,8 @@ void launch_prepare_table(const PrepareTable& tab, uint64_t ctas, uint64_t halo,
   cuda_check(cudaFuncSetAttribute(prepare_kernel<Batched>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)),
              "cudaFuncSetAttribute(prepare_kernel)");
-  prepare_kernel<Batched><<<static_cast<unsigned>(ctas), kThreads, smem, s>>>(tab);
+  const dim3 grid(static_cast<unsigned>(ctas), Batched ? 1u : tab.one.nseries);
+  prepare_kernel<Batched><<<grid, kThreads, smem, s>>>(tab);
   cuda_check(cudaGetLastError(), "prepare_kernel launch");
 }
 
@@ -1290,7 +1295,8 @@ void launch_prepare(const gf_ffa_program* P, const FfaMember& M, const float* de
   DeviceGuard dg(P->device);
   PrepareTable tab{};
   tab.one = prepare_item(M, dev_series, nseries, stride, dev_stats, dev_prepared);
-  launch_prepare_table<false>(tab, prepare_ctas(tab.one), M.halo, s);
+  check_arg(nseries < 65536, "nseries out of range");
+  launch_prepare_table<false>(tab, ceil_div(M.nsamples, kPrepareChunk), M.halo, s);
 }
 
 // One launch per class; batched programs walk their item runs.

@@ -57,7 +57,16 @@ struct PrepItem {
 
 enum PrepStage { kScrunch = 0, kMedian, kDetrend, kStats, kStages };
 
-// CTAs of an item in each stage's launch.
+// x blocks per series of the scrunch and detrend stages (1 for the others).
+uint64_t stage_xblocks(const PrepItem& it, int stage) {
+  switch (stage) {
+    case kScrunch: return it.factor > 1 ? ceil_div(it.low_n, 128) : 0;
+    case kDetrend: return ceil_div(it.n, 256);
+    default: return 1;
+  }
+}
+
+// CTAs of an item in each stage's batched launch.
 uint64_t stage_ctas(const PrepItem& it, int stage) {
   switch (stage) {
     case kScrunch: return it.factor > 1 ? ceil_div(it.low_n, 128) * it.nseries : 0;
@@ -104,20 +113,9 @@ __device__ __forceinline__ const PrepItem& cta_item(const PrepTable& t, int stag
 
 // low[s][k] = float(double sum of x[kF .. kF+F) / F); 128 outputs per CTA,
 // staged 32 samples at a time so global loads stay coalesced.
-template <bool Batched>
-__global__ void __launch_bounds__(128) scrunch_kernel(const __grid_constant__ PrepTable tab) {
-  __shared__ PrepItem sit;
-  __shared__ uint32_t sloc;
-  uint32_t local;
-  const PrepItem& it = cta_item<Batched>(tab, kScrunch, sit, sloc, local);
-  __shared__ float tile[128][33];
-  const uint32_t xblocks = static_cast<uint32_t>(ceil_div(it.low_n, 128));
-  const uint64_t s = local / xblocks;
-  const uint64_t k0 = static_cast<uint64_t>(local % xblocks) * 128;
+template <bool U32>
+__device__ __forceinline__ void scrunch_cta(const PrepItem& it, uint64_t s, uint64_t k0, float (*tile)[33]) {
   const uint64_t factor = it.factor, low_n = it.low_n;
-  const bool u32 = it.u32 != 0;
-  float* const low = it.low;
-  const uint64_t low_stride = it.low_stride;
   const char* row = static_cast<const char*>(it.series) + s * it.stride * 4;
   double acc = 0.0;
   for (uint64_t i0 = 0; i0 < factor; i0 += 32) {
@@ -127,7 +125,7 @@ __global__ void __launch_bounds__(128) scrunch_kernel(const __grid_constant__ Pr
       const int r = e >> 5, c = e & 31;
       const uint64_t k = k0 + r;
       float v = 0.0f;
-      if (k < low_n && c < cols) v = load_sample_ro(row, k * factor + i0 + c, u32);
+      if (k < low_n && c < cols) v = load_sample_ro(row, k * factor + i0 + c, U32);
       tile[r][c] = v;
     }
     __syncthreads();
@@ -136,7 +134,29 @@ __global__ void __launch_bounds__(128) scrunch_kernel(const __grid_constant__ Pr
       for (int c = 0; c < cols; ++c) acc = __dadd_rn(acc, static_cast<double>(tile[threadIdx.x][c]));
   }
   const uint64_t k = k0 + threadIdx.x;
-  if (k < low_n) low[s * low_stride + k] = static_cast<float>(__ddiv_rn(acc, static_cast<double>(factor)));
+  if (k < low_n) it.low[s * it.low_stride + k] = static_cast<float>(__ddiv_rn(acc, static_cast<double>(factor)));
+}
+
+template <bool Batched>
+__global__ void __launch_bounds__(128) scrunch_kernel(const __grid_constant__ PrepTable tab) {
+  __shared__ PrepItem sit;
+  __shared__ uint32_t sloc;
+  uint32_t local;
+  const PrepItem& it = cta_item<Batched>(tab, kScrunch, sit, sloc, local);
+  uint64_t s, k0;
+  if (Batched) {
+    const uint32_t xblocks = static_cast<uint32_t>(ceil_div(it.low_n, 128));
+    s = local / xblocks;
+    k0 = static_cast<uint64_t>(local % xblocks) * 128;
+  } else {
+    s = blockIdx.y;
+    k0 = static_cast<uint64_t>(blockIdx.x) * 128;
+  }
+  __shared__ float tile[128][33];
+  if (it.u32)
+    scrunch_cta<true>(it, s, k0, tile);
+  else
+    scrunch_cta<false>(it, s, k0, tile);
 }
 
 // Exact running median (window w odd) of an edge-padded series, one warp per
@@ -231,9 +251,15 @@ __global__ void __launch_bounds__(256) detrend_kernel(const __grid_constant__ Pr
   __shared__ uint32_t sloc;
   uint32_t local;
   const PrepItem& it = cta_item<Batched>(tab, kDetrend, sit, sloc, local);
-  const uint32_t xblocks = static_cast<uint32_t>(ceil_div(it.n, 256));
-  const uint64_t s = local / xblocks;
-  const uint64_t i = static_cast<uint64_t>(local % xblocks) * 256 + threadIdx.x;
+  uint64_t s, i;
+  if (Batched) {
+    const uint32_t xblocks = static_cast<uint32_t>(ceil_div(it.n, 256));
+    s = local / xblocks;
+    i = static_cast<uint64_t>(local % xblocks) * 256 + threadIdx.x;
+  } else {
+    s = blockIdx.y;
+    i = static_cast<uint64_t>(blockIdx.x) * 256 + threadIdx.x;
+  }
   if (i >= it.n) return;
   const bool u32 = it.u32 != 0;
   char* row = static_cast<char*>(it.series) + s * it.stride * 4;
@@ -436,18 +462,21 @@ size_t median_smem(int w) {
   return static_cast<size_t>(kMedianWarps) * 2 * cap * sizeof(float);
 }
 
-// The four stages over a table whose stage grids are ctas[stage].
+// The four stages: a batched launch over a table whose stage grids are
+// ctas[stage] CTAs; a single one with (x blocks, series) grids for scrunch
+// and detrend (ctas[] then holds x blocks, and the series count is the item's).
 template <bool Batched>
 void launch_stages(const PrepTable& tab, const uint64_t (&ctas)[kStages], size_t med_smem, cudaStream_t s) {
   for (int st = 0; st < kStages; ++st)
     check_arg(ctas[st] < (1ull << 31), "preprocessing launch too large");
+  const unsigned ny = Batched ? 1u : tab.one.nseries;
   cuda_check(cudaFuncSetAttribute(running_median_kernel<Batched>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(med_smem)),
              "cudaFuncSetAttribute(median)");
-  if (ctas[kScrunch]) scrunch_kernel<Batched><<<static_cast<unsigned>(ctas[kScrunch]), 128, 0, s>>>(tab);
+  if (ctas[kScrunch]) scrunch_kernel<Batched><<<dim3(static_cast<unsigned>(ctas[kScrunch]), ny), 128, 0, s>>>(tab);
   running_median_kernel<Batched><<<static_cast<unsigned>(ctas[kMedian]), 32 * kMedianWarps, med_smem, s>>>(tab);
   cuda_check(cudaGetLastError(), "running median launch");
-  detrend_kernel<Batched><<<static_cast<unsigned>(ctas[kDetrend]), 256, 0, s>>>(tab);
+  detrend_kernel<Batched><<<dim3(static_cast<unsigned>(ctas[kDetrend]), ny), 256, 0, s>>>(tab);
   cuda_check(cudaGetLastError(), "detrend launch");
   stats_kernel<Batched><<<static_cast<unsigned>(ctas[kStats]), 32 * kStatsWarps, 0, s>>>(tab);
   cuda_check(cudaGetLastError(), "stats launch");
@@ -462,8 +491,10 @@ extern "C" int gf_preprocess_inplace(const gf_preprocess_desc* d, void* dev_seri
     check_arg(d != nullptr, "null argument");
     PrepTable tab{};
     tab.one = make_item(*d, dev_series, input_is_u32, nseries, stride, dev_workspace, dev_stats, dev_status);
+    check_arg(nseries < 65536, "at most 65535 series per call");
     uint64_t ctas[kStages];
-    for (int st = 0; st < kStages; ++st) ctas[st] = stage_ctas(tab.one, st);
+    for (int st = 0; st < kStages; ++st)
+      ctas[st] = (st == kScrunch || st == kDetrend) ? stage_xblocks(tab.one, st) : stage_ctas(tab.one, st);
     launch_stages<false>(tab, ctas, median_smem(tab.one.w), as_stream(stream));
   });
 }
