@@ -402,7 +402,8 @@ def batched_measurement(nobs: int, device_id: int, case: str = "reduced") -> dic
         return time.perf_counter() - a, out
 
     sec_replay, got = timed(lambda: bs.run())         # staged data resident: graph replays only
-    sec_b, _ = timed(lambda: bs.run(data))           # with the staging of every filterbank
+    split = {}
+    sec_b, _ = timed(lambda: bs.run(data, timers=split))  # with the staging of every filterbank
     searches = [search.from_config(c, device_id=device_id) for c in cs]
     for s, x in zip(searches, data):
         s.run(x)                                     # warm-up
@@ -417,6 +418,7 @@ def batched_measurement(nobs: int, device_id: int, case: str = "reduced") -> dic
             "kernel_launches_per_run": launches, "seconds": sec_b, "seconds_staged_data": sec_replay,
             "sequential_value": units / sec_s, "sequential_seconds": sec_s, "speedup_vs_sequential": sec_s / sec_b,
             "identical_to_sequential": bool(same), "setup_seconds": setup,
+            "split_seconds": {k: round(v, 4) for k, v in split.items()},
             "tuned_dedispersion_shapes": tuner.cache, "case": case, "laws": BATCHED_CASES[case]}
 
 

@@ -28,8 +28,10 @@ sums are combined by atomics in a run-dependent order).
 """
 from __future__ import annotations
 
+import concurrent.futures as cf
 import dataclasses
 import json
+import os
 import math
 import time
 from pathlib import Path
@@ -152,7 +154,7 @@ class BatchSearch:
     and returns one search.SearchResult per observation."""
 
     def __init__(self, configs, device_id: int = 0, wave_bytes: int | None = None, tuner: Autotuner | None = None,
-                 use_graphs: bool = True, harmonic_options=None):
+                 use_graphs: bool = True, harmonic_options=None, finish_threads: int | None = None):
         self.configs = list(configs)
         if not self.configs:
             raise ValueError("a batch needs at least one observation")
@@ -163,6 +165,8 @@ class BatchSearch:
             if c.dedispersion != "brute" or c.obs.nbits != 8:
                 raise ValueError("batched search takes 8-bit brute-force observations")
         self.snr_threshold = thr.pop()
+        # host threads for the per-observation steps after the search
+        self.finish_threads = finish_threads or max(1, min(len(self.configs), os.cpu_count() or 1, 16))
         self.device = torch.device("cuda", device_id)
         self.device_id = device_id
         self.use_graphs = use_graphs
@@ -305,20 +309,42 @@ class BatchSearch:
             self._build_waves()
         t1 = time.perf_counter()
         parts = [[] for _ in self.configs]
-        for w in self.waves:
-            self._run_wave(w)
-            rec = w.ffa.collect(self.snr_threshold, rerun=lambda w=w: self._rerun_wave(w))
-            peaks, member = w.ffa.expand(rec, [pc.dm_begin for pc in w.pieces],
-                                         [self.configs[pc.obs].dm_low for pc in w.pieces],
-                                         [self.configs[pc.obs].dm_step for pc in w.pieces])
-            for m, pc in enumerate(w.pieces):
-                parts[pc.obs].append(peaks[member == m])
-        for pre in self.pre:
-            pre.synchronize()
-        for dd in self.dd:
-            dd.check()
-        t2 = time.perf_counter()
-        results = [self._finish(i, c, parts[i]) for i, c in enumerate(self.configs)]
+        last_wave = {}
+        for wi, w in enumerate(self.waves):
+            for pc in w.pieces:
+                last_wave[pc.obs] = wi
+        # An observation's host steps (sort, candidates, harmonics, fold) run
+        # on worker threads (the library releases the GIL inside its calls).
+        # When every wave replays a captured graph, an observation starts as
+        # soon as its last wave is collected, while the next waves run; a run
+        # that captures graphs starts them after the last wave, because work
+        # from other threads during a capture would invalidate it.
+        overlap = not self.use_graphs or all(w.graph is not None for w in self.waves)
+        futures = [None] * len(self.configs)
+        ready = []
+        with cf.ThreadPoolExecutor(max_workers=self.finish_threads) as pool:
+            for wi, w in enumerate(self.waves):
+                self._run_wave(w)
+                rec = w.ffa.collect(self.snr_threshold, rerun=lambda w=w: self._rerun_wave(w))
+                peaks, member = w.ffa.expand(rec, [pc.dm_begin for pc in w.pieces],
+                                             [self.configs[pc.obs].dm_low for pc in w.pieces],
+                                             [self.configs[pc.obs].dm_step for pc in w.pieces])
+                for m, pc in enumerate(w.pieces):
+                    parts[pc.obs].append(peaks[member == m])
+                    if last_wave[pc.obs] == wi:
+                        ready.append(pc.obs)
+                if overlap:
+                    for i in ready:
+                        futures[i] = pool.submit(self._finish, i, self.configs[i], parts[i])
+                    ready = []
+            for i in ready:
+                futures[i] = pool.submit(self._finish, i, self.configs[i], parts[i])
+            t2 = time.perf_counter()
+            for pre in self.pre:
+                pre.synchronize()
+            for dd in self.dd:
+                dd.check()
+            results = [f.result() for f in futures]
         t3 = time.perf_counter()
         if timers is not None:
             timers.update(setup=t1 - t0, search=t2 - t1, finish=t3 - t2, total=t3 - t0)
