@@ -333,12 +333,26 @@ __global__ void __launch_bounds__(32 * kStatsWarps) stats_kernel(const __grid_co
     cp_async_wait_1();
     __syncwarp();
     if (lane == 0) {
-      const float* b = buf[warp][c & 1];
-      const uint64_t len = umin64(kStatsChunk, nvec * 4 - c * kStatsChunk);
-      for (uint64_t i = 0; i < len; ++i) {
-        const double a = b[i];
-        sum = __dadd_rn(sum, a);
-        sq = __dadd_rn(sq, __dmul_rn(a, a));
+      // four samples per vector load, the next vector loaded and the squares
+      // formed ahead of the two dependent add chains (same order as one at a
+      // time; len is a multiple of 4)
+      const float4* b4 = reinterpret_cast<const float4*>(buf[warp][c & 1]);
+      const uint32_t nv = static_cast<uint32_t>(umin64(kStatsChunk, nvec * 4 - c * kStatsChunk) / 4);
+      float4 nxt = b4[0];
+      for (uint32_t v = 0; v < nv; ++v) {
+        const float4 cur = nxt;
+        if (v + 1 < nv) nxt = b4[v + 1];
+        const double a0 = cur.x, a1 = cur.y, a2 = cur.z, a3 = cur.w;
+        const double q0 = __dmul_rn(a0, a0), q1 = __dmul_rn(a1, a1), q2 = __dmul_rn(a2, a2),
+                     q3 = __dmul_rn(a3, a3);
+        sum = __dadd_rn(sum, a0);
+        sq = __dadd_rn(sq, q0);
+        sum = __dadd_rn(sum, a1);
+        sq = __dadd_rn(sq, q1);
+        sum = __dadd_rn(sum, a2);
+        sq = __dadd_rn(sq, q2);
+        sum = __dadd_rn(sum, a3);
+        sq = __dadd_rn(sq, q3);
       }
     }
     __syncwarp();
