@@ -436,8 +436,47 @@ def evaluate(scorer, examples, fractions, dm_max: float) -> dict:
     return out
 
 
+def evaluate_held_out(cfg, nobs: int, seed: int, dm_max: float, coarse_cost: float | None) -> dict:
+    """Recall of the shipped weights, the max-coarse-S/N heuristic and random
+    windows on nobs held-out seeded observations (seeds 20000 + seed + i, never
+    used for training or validation), at every window fraction, with the
+    speed-up over the exhaustive search that each fraction implies:
+    1 / (coarse_cost + fraction).  coarse_cost defaults to the measured cost
+    of the coarse search and network on the first observation."""
+    import time
+    held, ds, cf = make_examples(cfg, range(20_000 + seed, 20_000 + seed + nobs))
+    net = ProposalNet()
+    meta = net.load_default()
+    if coarse_cost is None:
+        obs = synthetic_observation(20_000 + seed, cfg.obs.nchans, cfg.obs.nsamples, cfg.obs.tsamp, cfg.obs.f_low,
+                                    cfg.obs.f_high, dm_max)
+        raw = core.synth_generate(obs)
+        ds.run(raw)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ds.run(raw)
+        torch.cuda.synchronize()
+        t_full = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        net.forward(cf(raw))
+        torch.cuda.synchronize()
+        coarse_cost = (time.perf_counter() - t0) / t_full
+    fractions = [k / NCOARSE for k in range(1, NCOARSE + 1)]
+    rec = evaluate(lambda e: net.forward(e.features), held, fractions, dm_max)
+    base = evaluate(lambda e: baseline_scores(e.features), held, fractions, dm_max)
+    rng = np.random.default_rng(seed)
+    rand = evaluate(lambda e: torch.from_numpy(rng.random((NCOARSE, 1))), held, fractions, dm_max)
+    curve = {f"{f:.4f}": {"speedup": 1.0 / (coarse_cost + f), "trained": rec[f], "heuristic": base[f],
+                          "random": rand[f]} for f in fractions}
+    out = {"held_out_observations": nobs, "detected_injections": rec[fractions[-1]][1],
+           "coarse_cost": coarse_cost, "weights": meta.get("trained_on", ""), "curve": curve}
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def main() -> None:
     """python -m gaffa_b200.proposal train [--train N] [--val M] [--nsamples-log2 L] [--epochs E] [--out PATH]
+    python -m gaffa_b200.proposal evaluate [--val M]   (held-out recall curve of the shipped weights)
 
     Generates seeded survey-band injections (4096 channels, 1100-1700 MHz,
     DMs 0-1000 in 2048 trials, 2^L samples), labels them with the exhaustive
@@ -449,7 +488,7 @@ def main() -> None:
 
     from . import configs
     ap = argparse.ArgumentParser()
-    ap.add_argument("command", choices=["train"])
+    ap.add_argument("command", choices=["train", "evaluate"])
     ap.add_argument("--train", type=int, default=100)
     ap.add_argument("--val", type=int, default=20)
     ap.add_argument("--nsamples-log2", type=int, default=20)
@@ -458,9 +497,14 @@ def main() -> None:
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=str(DEFAULT_WEIGHTS))
+    ap.add_argument("--coarse-cost", type=float, default=None,
+                    help="evaluate: cost of the coarse search and network as a fraction of the exhaustive search")
     a = ap.parse_args()
     cfg = configs.survey_size(nsamples=1 << a.nsamples_log2)
     dm_max = cfg.dm_low + (cfg.ndm - 1) * cfg.dm_step
+    if a.command == "evaluate":
+        evaluate_held_out(cfg, a.val, a.seed, dm_max, a.coarse_cost)
+        return
     t0 = time.time()
     train_set, ds, cf = make_examples(cfg, range(a.seed, a.seed + a.train))
     val_set, _, _ = make_examples(cfg, range(10_000 + a.seed, 10_000 + a.seed + a.val), ds=ds, cf=cf)
