@@ -13,8 +13,8 @@
 // derived from the exhaustive search's candidates.
 //
 // This component has no counterpart in the reference: the exhaustive search
-// (every other file of this library) stays the fallback and the judge of its
-// recall.
+// (every other file of this library) stays the fallback and the measure of
+// its recall.
 #include <cuda_bf16.h>
 
 #include "common.cuh"

@@ -15,7 +15,7 @@ injected pulsar (its period or a harmonic ratio n/m, n, m <= 4, at a DM whose
 smearing stays below a quarter period) are positive.  At inference the
 windows are ranked by their best octave score and only the top fraction goes
 to the full-resolution search (DmSearch.run(dm_ranges=...)); the exhaustive
-search remains the fallback and the judge of recall.
+search remains the fallback and the measure of recall.
 """
 from __future__ import annotations
 

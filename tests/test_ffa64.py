@@ -1,6 +1,6 @@
 """The FP64 restatement of the FFA search (oracle/ffa64_oracle.c) against the
 bit-exact FP32 one (oracle/gaffa_oracle.c): transform rows and boxcar S/N of
-every evaluated row and width agree within the north-star tolerance of 1e-5
+every evaluated row and width agree within the specified tolerance of 1e-5
 relative (absolute below |S/N| = 1, where a relative bound means nothing)."""
 import sys
 from pathlib import Path
