@@ -34,10 +34,20 @@ int main(void) {
     printf("task %llu bins %llu rows %llu rows_eval %llu factor %.17g\n", (unsigned long long)i,
            (unsigned long long)tasks[i].bins, (unsigned long long)tasks[i].rows,
            (unsigned long long)tasks[i].rows_eval, tasks[i].downsample_factor);
+  /* batched launches and the copy-ring status: null arguments are
+     rejected before any CUDA call */
+  gf_preprocess_batch* pb = NULL;
+  int bad = 0;
+  bad |= gf_preprocess_batch_create(NULL, 1, 0, &pb) != GF_EINVAL;
+  bad |= gf_preprocess_batch_run(NULL, NULL) != GF_EINVAL;
+  bad |= gf_ffa_batch_prepare_all(NULL, NULL) != GF_EINVAL;
+  bad |= gf_ffa_batch_bind_series(NULL, NULL, NULL, NULL) != GF_EINVAL;
+  bad |= gf_dedisp_check(NULL, NULL) != GF_EINVAL;
+  printf("batched entry points reject null arguments: %s\n", bad ? "no" : "yes");
   uint64_t n = 0;
   const int rc = gf_downsampled_size(100, 0.5, &n); /* factor < 1: rejected */
   printf("error %d %s\n", rc, gf_last_error());
   free(tasks);
   free(widths);
-  return rc == GF_EINVAL ? 0 : 2;
+  return rc == GF_EINVAL && !bad ? 0 : 2;
 }
