@@ -14,23 +14,25 @@
 // streams channel chunks through a ring of 2-4 shared-memory stages: for each
 // channel of a chunk one bulk copy (cp.async.bulk, completion counted in bytes
 // on the stage's mbarrier) brings the window [t0 + base, t0 + base + RS)
-// (base = delay of the block's first DM rounded down to 16), and one more per
-// DM its gather records.  Warps wait on the stage's barrier, sum, and release
-// the stage with an acquire-release counter; the last warp to release it
-// issues the copies of the chunk `stages` ahead into it.  No CTA-wide barrier
-// runs per chunk, so warps drift apart by up to `stages` chunks.  DM blocks
-// are the fastest grid index, so the CTAs resident at one time cover a few
-// time tiles of every DM block of the launch and read each input window from
-// L2.  A warp reads its DM's shifted
-// window as aligned 32-bit words: the delay offset off = d - base splits into a
-// word offset q = off >> 2 and a byte class s = off & 3.  The host sorts each
-// warp's channels by class, so the class is static inside the loop: a word
-// holds 4 consecutive input bytes, which are split into even/odd byte pairs
-// (LOP3 and PRMT) and accumulated in 16-bit lanes by IMAD; a class with an
-// odd channel count ends with one single-channel step.  Per 256 channels the
-// 16-bit lanes are flushed into 32-bit sums, realigning class s by s bytes
-// with one lane shuffle.  Lanes read consecutive words, so every LDS.32 is
-// conflict-free.
+// (base = delay of the block's first DM rounded down to 16), one more per DM
+// its gather records, and one more the window bases of the chunk `stages`
+// ahead.  Warps wait on the stage's barrier, sum, and release the stage with
+// an acquire-release counter; the last warp to release it issues the copies
+// of the chunk `stages` ahead into it, reading that chunk's window bases from
+// the stage (so the refilling warp never waits on global memory).  No
+// CTA-wide barrier runs per chunk, so warps drift apart by up to `stages`
+// chunks.  DM blocks are the fastest grid index, so the CTAs resident at one
+// time cover a few time tiles of every DM block of the launch and read each
+// input window from L2.  A warp reads its DM's shifted window as aligned
+// 32-bit words: the delay offset off = d - base splits into a word offset
+// q = off >> 2 and a byte class s = off & 3.  The host sorts each warp's
+// channels by class, so the class is static inside the loop: a word holds 4
+// consecutive input bytes, which are split into even/odd byte pairs (LOP3 and
+// PRMT) and accumulated in 16-bit lanes by IMAD; a class with an odd channel
+// count ends with one single-channel step.  Per 256 channels the 16-bit lanes
+// are flushed into 32-bit sums kept in shared memory after the ring,
+// realigning class s by s bytes with one lane shuffle.  Lanes read
+// consecutive words, so every LDS.32 is conflict-free.
 #include "common.cuh"
 
 #include <algorithm>
