@@ -10,6 +10,12 @@ pinned host filterbank (host->device copy inside the timed region).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gaffa|reference]
 
+The same line carries measurements of the other workloads on rank 0: the
+learned proposal, two batched uneven workloads, the wide-range subband
+configuration at its size (`--no-proposal`, `--no-batched`,
+`--no-wide-subband` skip them), and, with `--batched-configured`, the
+batched workload at its configured laws (64 observations, ~20 minutes).
+
 Multi-GPU runs (torchrun) are replicas: every rank searches its own
 observation (weak scaling); time is the max over ranks.  `--impl reference`
 times the reference's own CPU implementation (compiled from its sources,
