@@ -33,6 +33,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <tuple>
 #include <vector>
 
 namespace cg = cooperative_groups;
@@ -40,10 +41,13 @@ namespace cg = cooperative_groups;
 namespace gf {
 namespace {
 
-// One 1024-thread CTA per SM for the search (222 KB of shared memory: larger
-// subtrees and column blocks than two 512-thread CTAs with 110 KB each, and
-// 2.5 % faster on the survey plan); 512 threads for the prepare pass.
+// Search CTAs: tasks that fit one 512-thread CTA's tiles (110 KB, two CTAs
+// per SM, more items in flight) run there; larger tasks run on one
+// 1024-thread CTA per SM (222 KB: larger subtrees and column blocks, 2.5 %
+// faster on the survey plan than two 512-thread CTAs).  512 threads for the
+// prepare pass.
 constexpr int kThreads = 1024;
+constexpr int kSmallThreads = 512;
 constexpr int kPrepareThreads = 512;
 constexpr int kMaxBins = 512;
 constexpr int kMaxWidths = 64;
@@ -308,7 +312,7 @@ struct PassDev {
   uint32_t block_begin, nblocks;
 };
 
-constexpr int kWarps = kThreads / 32;
+// Search-path device functions take the CTA size T (512 or 1024 threads).
 
 // Dynamic shared memory of the search kernel: two ColBlock headers, the
 // staged schedule, then two row buffers.
@@ -332,12 +336,12 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // lane j handles bins j, j+32, ...; only the last iteration can be partial.
 // The tail row is read at k = (j + roll) mod bins, computed branch-free as
 // min(k, k - bins) in unsigned arithmetic (k < 2 bins).
-template <int NB>
+template <int NB, int T>
 __device__ __forceinline__ void merge_level(const MetaEntry* meta, uint32_t nrows, const float* prev, float* out,
                                             uint32_t pitch, uint32_t bins) {
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool last_ok = lane + 32u * (NB - 1) < bins;
-  for (uint32_t q = warp; q < nrows; q += kWarps) {
+  for (uint32_t q = warp; q < nrows; q += T / 32) {
     const MetaEntry m = meta[q];
     float* o = out + q * pitch + lane;
     const float* h = prev + m.a * pitch + lane;
@@ -363,12 +367,12 @@ __device__ __forceinline__ void merge_level(const MetaEntry* meta, uint32_t nrow
 }
 
 // rows [0, n) of read-only global `src` (row length bins) into smem, async
-template <int NB>
+template <int NB, int T>
 __device__ __forceinline__ void load_rows_async(const float* src, uint32_t n, uint32_t bins, float* out,
                                                 uint32_t pitch) {
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool last_ok = lane + 32u * (NB - 1) < bins;
-  for (uint32_t q = warp; q < n; q += kWarps) {
+  for (uint32_t q = warp; q < n; q += T / 32) {
     const float* g = src + static_cast<uint64_t>(q) * bins + lane;
     float* o = out + q * pitch + lane;
 #pragma unroll
@@ -377,11 +381,11 @@ __device__ __forceinline__ void load_rows_async(const float* src, uint32_t n, ui
   }
 }
 
-template <int NB>
+template <int NB, int T>
 __device__ __forceinline__ void store_rows(const float* in, uint32_t pitch, uint32_t n, uint32_t bins, float* dst) {
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool last_ok = lane + 32u * (NB - 1) < bins;
-  for (uint32_t q = warp; q < n; q += kWarps) {
+  for (uint32_t q = warp; q < n; q += T / 32) {
     float* g = dst + static_cast<uint64_t>(q) * bins + lane;
     const float* s = in + q * pitch + lane;
 #pragma unroll
@@ -420,7 +424,7 @@ __device__ __forceinline__ float key_float(uint32_t k) {
 // row maximum, from which S/N follows (:141-170).  Only when S/N passes the
 // threshold is the first phase attaining the maximum looked up (the
 // reference's strict '>' scan keeps the first maximum), and a peak appended.
-template <int NB>
+template <int NB, int T>
 __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, uint32_t shift0, float* cp,
                             uint32_t cp_pitch, const DetectArgs& a) {
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -457,7 +461,7 @@ __device__ void detect_rows(const float* rows, uint32_t pitch, uint32_t count, u
   }
   __syncthreads();
   const bool last_ok = lane + 32u * (NB - 1) < bins;
-  for (uint32_t r = warp; r < count; r += kWarps) {
+  for (uint32_t r = warp; r < count; r += T / 32) {
     const float* c = cp + r * cp_pitch + lane;
     float base[NB];
 #pragma unroll
@@ -556,18 +560,18 @@ __device__ __forceinline__ DetectArgs make_detect(const SearchParams& p, const T
 // input row) from its input rows up to relative level `stop` (0: the
 // subtree root).  The subtree's schedule (depth x n entries, level depth-1
 // first) is left in cmeta.  Returns the buffer holding level `stop`.
-template <int NB>
+template <int NB, int T>
 __device__ float* eval_subtree(const SearchParams& p, const float* src, uint32_t n, uint32_t bins, uint32_t stop,
                                float* buf0, float* buf1, MetaEntry* cmeta) {
   const uint32_t pitch = p.pitch;
   const uint32_t md = tree_depth(n);
   const MetaEntry* table = p.sub_meta + p.sub_offset[n];
-  for (uint32_t e = threadIdx.x; e < md * n; e += kThreads) cp_async8(cmeta + e, table + e);
-  load_rows_async<NB>(src, n, bins, (md & 1) ? buf1 : buf0, pitch);
+  for (uint32_t e = threadIdx.x; e < md * n; e += T) cp_async8(cmeta + e, table + e);
+  load_rows_async<NB, T>(src, n, bins, (md & 1) ? buf1 : buf0, pitch);
   cp_async_wait_all();
   __syncthreads();
   for (int l = static_cast<int>(md) - 1; l >= static_cast<int>(stop); --l) {
-    merge_level<NB>(cmeta + (md - 1 - l) * n, n, ((l + 1) & 1) ? buf1 : buf0, (l & 1) ? buf1 : buf0, pitch, bins);
+    merge_level<NB, T>(cmeta + (md - 1 - l) * n, n, ((l + 1) & 1) ? buf1 : buf0, (l & 1) ? buf1 : buf0, pitch, bins);
     __syncthreads();
   }
   return (stop & 1) ? buf1 : buf0;
@@ -576,7 +580,7 @@ __device__ float* eval_subtree(const SearchParams& p, const float* src, uint32_t
 // Column block `hb`: stages its merge entries, loads its bottom rows from
 // `src` (scratch written by the cluster's CTAs in the previous phase),
 // evaluates its levels.  The output rows (hb.count[0]) end in buf0.
-template <int NB>
+template <int NB, int T>
 __device__ void eval_block(const SearchParams& p, const ColBlock& hb, const float* src, uint32_t bins, float* buf0,
                            float* buf1, MetaEntry* cmeta) {
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -585,7 +589,7 @@ __device__ void eval_block(const SearchParams& p, const ColBlock& hb, const floa
   uint32_t nmeta = 0;
   for (uint32_t k = 0; k < K; ++k) nmeta += hb.count[k];
   const MetaEntry* gm = p.col_meta + hb.meta;  // 16-byte aligned, padded to an even count
-  for (uint32_t e = 2 * threadIdx.x; e < nmeta; e += 2 * kThreads) cp_async16(cmeta + e, gm + e);
+  for (uint32_t e = 2 * threadIdx.x; e < nmeta; e += 2 * T) cp_async16(cmeta + e, gm + e);
   float* bottom = (K & 1) ? buf1 : buf0;
   const uint32_t nb = hb.count[K];
   const uint32_t nruns = hb.nruns;
@@ -593,7 +597,7 @@ __device__ void eval_block(const SearchParams& p, const ColBlock& hb, const floa
   // Bottom rows: async copies, all in flight at once.  The rows were written
   // by other CTAs of the cluster before the cluster barrier, whose acquire
   // makes them visible to these (L1-allocating) reads.
-  for (uint32_t q = warp; q < nb; q += kWarps) {
+  for (uint32_t q = warp; q < nb; q += T / 32) {
     uint32_t j = 0;  // run holding buffer row q (runs ascend in run_off)
 #pragma unroll
     for (uint32_t r = 1; r < 8; ++r) j += (r < nruns && hb.run_off[r] <= q) ? 1u : 0u;
@@ -607,7 +611,7 @@ __device__ void eval_block(const SearchParams& p, const ColBlock& hb, const floa
   __syncthreads();
   uint32_t off = 0;
   for (int k = static_cast<int>(K) - 1; k >= 0; --k) {
-    merge_level<NB>(cmeta + off, hb.count[k], ((k + 1) & 1) ? buf1 : buf0, (k & 1) ? buf1 : buf0, pitch, bins);
+    merge_level<NB, T>(cmeta + off, hb.count[k], ((k + 1) & 1) ? buf1 : buf0, (k & 1) ? buf1 : buf0, pitch, bins);
     off += hb.count[k];
     __syncthreads();
   }
@@ -622,8 +626,8 @@ __device__ __forceinline__ void load_header(ColBlock* dst, const ColBlock* src) 
 // One (series, task) per cluster (cluster size 1, 2, 4 or 8); items are
 // task-major so the series of one task run together.  NB = ceil(bins/32)
 // of every task of the launch.
-template <int NB>
-__global__ void __launch_bounds__(kThreads, 1) ffa_search_kernel(SearchParams p) {
+template <int NB, int T>
+__global__ void __launch_bounds__(T, T <= 512 ? 2 : 1) ffa_search_kernel(SearchParams p) {
   cg::cluster_group cluster = cg::this_cluster();
   const uint32_t cs = cluster.num_blocks();
   const uint32_t rank = cluster.block_rank();
@@ -668,23 +672,23 @@ __global__ void __launch_bounds__(kThreads, 1) ffa_search_kernel(SearchParams p)
     if (dS == 0) {
       // whole task on chip: levels below the root, then root rows in batches
       if (t.rows == 1) {
-        load_rows_async<NB>(input, 1, bins, buf0, pitch);
+        load_rows_async<NB, T>(input, 1, bins, buf0, pitch);
         cp_async_wait_all();
         __syncthreads();
-        detect_rows<NB>(buf0, pitch, 1, 0, buf1, cp_pitch, da);
+        detect_rows<NB, T>(buf0, pitch, 1, 0, buf1, cp_pitch, da);
         __syncthreads();  // the width scans read buf1 until here; the next item loads into it
         continue;
       }
-      float* lvl1 = eval_subtree<NB>(p, input, t.rows, bins, 1, buf0, buf1, cmeta);
+      float* lvl1 = eval_subtree<NB, T>(p, input, t.rows, bins, 1, buf0, buf1, cmeta);
       float* other = lvl1 == buf0 ? buf1 : buf0;
       const uint32_t md = tree_depth(t.rows);
       const MetaEntry* root = cmeta + (md - 1) * t.rows;
-      const uint32_t batch = umin32(kThreads, (p.max_rows * pitch) / (pitch + cp_pitch));
+      const uint32_t batch = umin32(T, (p.max_rows * pitch) / (pitch + cp_pitch));
       for (uint32_t b0 = 0; b0 < t.rows_eval; b0 += batch) {
         const uint32_t cnt = umin32(batch, t.rows_eval - b0);
-        merge_level<NB>(root + b0, cnt, lvl1, other, pitch, bins);
+        merge_level<NB, T>(root + b0, cnt, lvl1, other, pitch, bins);
         __syncthreads();
-        detect_rows<NB>(other, pitch, cnt, b0, other + batch * pitch, cp_pitch, da);
+        detect_rows<NB, T>(other, pitch, cnt, b0, other + batch * pitch, cp_pitch, da);
       }
       __syncthreads();  // the last width scans read `other` until here; the next item loads into it
       continue;
@@ -693,9 +697,9 @@ __global__ void __launch_bounds__(kThreads, 1) ffa_search_kernel(SearchParams p)
     const uint32_t nsub = 1u << dS;
     for (uint32_t sub = rank; sub < nsub; sub += cs) {
       const Node nd = node_at(sub, t.rows, dS);
-      const float* res = eval_subtree<NB>(p, input + static_cast<uint64_t>(nd.a) * bins, nd.n, bins, 0, buf0, buf1,
+      const float* res = eval_subtree<NB, T>(p, input + static_cast<uint64_t>(nd.a) * bins, nd.n, bins, 0, buf0, buf1,
                                           cmeta);
-      store_rows<NB>(res, pitch, nd.n, bins, q0 + static_cast<uint64_t>(nd.a) * bins);
+      store_rows<NB, T>(res, pitch, nd.n, bins, q0 + static_cast<uint64_t>(nd.a) * bins);
       __syncthreads();
     }
     cluster.sync();
@@ -712,12 +716,12 @@ __global__ void __launch_bounds__(kThreads, 1) ffa_search_kernel(SearchParams p)
       for (uint32_t u = rank; u < pd.nblocks; u += cs, ++it) {
         const ColBlock& hb = hdr[it & 1];
         if (u + cs < pd.nblocks) load_header(&hdr[(it + 1) & 1], blocks + u + cs);
-        eval_block<NB>(p, hb, src, bins, buf0, buf1, cmeta);
+        eval_block<NB, T>(p, hb, src, bins, buf0, buf1, cmeta);
         if (hb.final_pass) {
-          detect_rows<NB>(buf0, pitch, hb.count[0], hb.out_row, buf1, cp_pitch, da);
+          detect_rows<NB, T>(buf0, pitch, hb.count[0], hb.out_row, buf1, cp_pitch, da);
           __syncthreads();  // the width scans read buf1 until here; the next block may load into it
         } else {
-          store_rows<NB>(buf0, pitch, hb.count[0], bins, dst + static_cast<uint64_t>(hb.out_row) * bins);
+          store_rows<NB, T>(buf0, pitch, hb.count[0], bins, dst + static_cast<uint64_t>(hb.out_row) * bins);
           __syncthreads();
         }
       }
@@ -758,14 +762,19 @@ __global__ void __launch_bounds__(kThreads) ffa_level_kernel(const float* __rest
 
 using SearchKernel = void (*)(SearchParams);
 
-// ffa_search_kernel<NB> for NB = 1 .. 16 (bins <= 512)
-SearchKernel search_kernel_for(uint32_t nb) {
+// ffa_search_kernel<NB, T> for NB = 1 .. 16 (bins <= 512), T = 512 or 1024
+template <int T>
+SearchKernel search_kernel_table(uint32_t nb) {
   static const SearchKernel table[16] = {
-      ffa_search_kernel<1>,  ffa_search_kernel<2>,  ffa_search_kernel<3>,  ffa_search_kernel<4>,
-      ffa_search_kernel<5>,  ffa_search_kernel<6>,  ffa_search_kernel<7>,  ffa_search_kernel<8>,
-      ffa_search_kernel<9>,  ffa_search_kernel<10>, ffa_search_kernel<11>, ffa_search_kernel<12>,
-      ffa_search_kernel<13>, ffa_search_kernel<14>, ffa_search_kernel<15>, ffa_search_kernel<16>};
+      ffa_search_kernel<1, T>,  ffa_search_kernel<2, T>,  ffa_search_kernel<3, T>,  ffa_search_kernel<4, T>,
+      ffa_search_kernel<5, T>,  ffa_search_kernel<6, T>,  ffa_search_kernel<7, T>,  ffa_search_kernel<8, T>,
+      ffa_search_kernel<9, T>,  ffa_search_kernel<10, T>, ffa_search_kernel<11, T>, ffa_search_kernel<12, T>,
+      ffa_search_kernel<13, T>, ffa_search_kernel<14, T>, ffa_search_kernel<15, T>, ffa_search_kernel<16, T>};
   return table[nb - 1];
+}
+
+SearchKernel search_kernel_for(uint32_t nb, int threads) {
+  return threads == kSmallThreads ? search_kernel_table<kSmallThreads>(nb) : search_kernel_table<kThreads>(nb);
 }
 
 }  // namespace
@@ -783,6 +792,7 @@ struct FfaGeometry {
 
 struct FfaClass {
   int cluster = 1;             // CTAs cooperating on one (series, task)
+  int threads = kThreads;      // CTA size (kSmallThreads or kThreads)
   uint32_t nb = 1;             // ceil(bins / 32) of every task of the class
   SearchKernel kernel = nullptr;
   std::vector<uint32_t> tasks; // largest first
@@ -823,7 +833,7 @@ struct gf_ffa_program {
   std::vector<PassDev> passes;
   std::vector<FfaClass> classes;
   uint32_t max_bins = 0, max_width = 0;
-  FfaGeometry geo[17];         // by NB (1..16)
+  FfaGeometry geo[2][17];      // by CTA size (0: kSmallThreads, 1: kThreads) and NB (1..16)
   uint64_t max_series = 0;
   uint64_t scratch_floats = 0;
   DeviceBlob tasks_d, trials_d, sub_meta_d, sub_offset_d, col_meta_d, blocks_d, passes_d, members_d;
@@ -1113,13 +1123,15 @@ std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& spe
     P->task_member.insert(P->task_member.end(), s.ntasks, static_cast<uint32_t>(m));
     P->members.push_back(std::move(M));
   }
-  // shared-memory geometry per NB: two ColBlock headers, the staged
-  // schedule, two row buffers of max_rows rows of the class's widest rows;
-  // sized for one CTA per SM (227 KB per CTA at most, static state aside)
-  const size_t budget = 222 * 1024;
+  // shared-memory geometry per CTA size and NB: two ColBlock headers, the
+  // staged schedule, two row buffers of max_rows rows of the class's widest
+  // rows; sized for two 512-thread CTAs or one 1024-thread CTA per SM (227 KB
+  // per CTA at most, static state aside)
   uint32_t max_rows_all = 0;
+  for (int gi = 0; gi < 2; ++gi)
   for (uint32_t nb = 1; nb <= 16; ++nb) {
-    FfaGeometry& g = P->geo[nb];
+    const size_t budget = gi == 0 ? 110 * 1024 : 222 * 1024;
+    FfaGeometry& g = P->geo[gi][nb];
     const uint32_t cap = std::min<uint32_t>(32 * nb, P->max_bins);
     if (32 * (nb - 1) >= P->max_bins) break;
     g.pitch = cap | 1u;
@@ -1153,7 +1165,7 @@ std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& spe
   }
   if (P->sub_meta.empty()) P->sub_meta.push_back(MetaEntry{});
   // tasks, trials, column schedules and classes
-  std::map<std::pair<int, uint32_t>, size_t> class_of;
+  std::map<std::tuple<int, uint32_t, int>, size_t> class_of;
   for (uint64_t i = 0; i < P->tasks.size(); ++i) {
     const auto& t = P->tasks[i];
     const uint32_t m = P->task_member[i];
@@ -1179,7 +1191,9 @@ std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& spe
       P->trial_dev.push_back(TrialDev{h, wf / (bf - wf) * h, static_cast<uint32_t>(w), 0u});
     }
     const uint32_t nbt = static_cast<uint32_t>(ceil_div(t.bins, 32));
-    const FfaGeometry& g = P->geo[nbt];
+    // on chip in a 512-thread CTA when it fits, else the 1024-thread tiles
+    const int gi = t.rows <= P->geo[0][nbt].max_rows ? 0 : 1;
+    const FfaGeometry& g = P->geo[gi][nbt];
     uint32_t ds = 0;
     while (ceil_div(t.rows, 1ull << ds) > g.max_rows) ++ds;
     check_arg(ds <= 15, "FFA task too deep");
@@ -1192,13 +1206,15 @@ std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& spe
       while (cluster < kClusterSize && static_cast<uint64_t>(cluster) * 512 < t.rows) cluster *= 2;
     }
     const uint32_t nb = static_cast<uint32_t>(ceil_div(t.bins, 32));
-    const std::pair<int, uint32_t> key{ds == 0 ? 0 : cluster, nb};
+    const int threads = gi == 0 ? kSmallThreads : kThreads;
+    const std::tuple<int, uint32_t, int> key{ds == 0 ? 0 : cluster, nb, threads};
     if (!class_of.count(key)) {
       class_of[key] = P->classes.size();
       P->classes.emplace_back();
       P->classes.back().cluster = cluster;
+      P->classes.back().threads = threads;
       P->classes.back().nb = nb;
-      P->classes.back().kernel = search_kernel_for(nb);
+      P->classes.back().kernel = search_kernel_for(nb, threads);
     }
     FfaClass& c = P->classes[class_of[key]];
     c.tasks.push_back(static_cast<uint32_t>(i));
@@ -1224,7 +1240,7 @@ std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& spe
       }
       c.units_d.upload(c.units.data(), c.units.size() * sizeof(UnitDev), device_id);
     }
-    const FfaGeometry& g = P->geo[c.nb];
+    const FfaGeometry& g = P->geo[c.threads == kSmallThreads ? 0 : 1][c.nb];
     cuda_check(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(g.smem_bytes)),
                "cudaFuncSetAttribute(ffa_search_kernel)");
@@ -1232,7 +1248,7 @@ std::unique_ptr<gf_ffa_program> build_program(const std::vector<MemberSpec>& spe
                "cudaFuncSetAttribute(cluster size)");
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(c.cluster, 1, 1);
-    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.blockDim = dim3(static_cast<unsigned>(c.threads), 1, 1);
     cfg.dynamicSmemBytes = g.smem_bytes;
     cudaLaunchAttribute attr{};
     attr.id = cudaLaunchAttributeClusterDimension;
@@ -1337,7 +1353,7 @@ void launch_search(gf_ffa_program* P, const float* dev_prepared, uint64_t nserie
     sp.nunits = static_cast<uint32_t>(c.units.size());
     sp.nitems = c.nitems;
     sp.scratch_elems = c.max_elems;
-    const FfaGeometry& g = P->geo[c.nb];
+    const FfaGeometry& g = P->geo[c.threads == kSmallThreads ? 0 : 1][c.nb];
     sp.pitch = g.pitch;
     sp.max_rows = g.max_rows;
     sp.front = g.front;
@@ -1346,7 +1362,7 @@ void launch_search(gf_ffa_program* P, const float* dev_prepared, uint64_t nserie
     const unsigned nclusters = static_cast<unsigned>(std::min<uint64_t>(items, static_cast<uint64_t>(c.nclusters)));
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(nclusters * c.cluster, 1, 1);
-    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.blockDim = dim3(static_cast<unsigned>(c.threads), 1, 1);
     cfg.dynamicSmemBytes = g.smem_bytes;
     cfg.stream = s;
     cudaLaunchAttribute attr{};
